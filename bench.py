@@ -1,0 +1,372 @@
+"""Benchmark of the Kirchhoff engine (prints ONE JSON line on rank 0).
+
+Default workload: the single large solve — 2^20 rays on a Gaussian aperture
+(sigma 0.1 mm, R = 30 m, 10 keV) against a 512x512 screen grid of +-0.5 mm at
+z = 1000 mm (2.75e11 ray x screen pairs per step), FP32 phase-reduced form.
+
+  value  Gpair/s of the FP32 phase-reduced solve with inputs resident in HBM
+         (CUDA events on the launching stream, L2 flushed between steps)
+  e2e    the same through the host-buffer C ABI (pinned host inputs, H2D
+         copies, solve, D2H of the field), wall clock per step
+  fp64_plain  the plain FP64 solve on the same inputs (the 10x reference)
+  roofline    the pair kernel against the FP32-FMA/SFU pair roofline
+  cpu_baseline the CPU oracle (a restatement of src/waves/diffraction.rs) on
+         a bounded sample of screen points, all host threads
+
+`--impl reference` times the reference's CPU algorithm (the oracle port, the
+reference's Rust cannot be built here) on the same workload's sample.
+
+Multi-GPU (torchrun): every rank runs its own replica of the workload (weak
+scaling, no data-path collective); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "xrt-rs_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Gpair/s (ray x screen pair evaluations), FP32 phase-reduced vs FP64 plain"
+UNIT = "Gpair/s"
+# Algorithmic work per ray x screen pair of the reference formula
+# (kirchhoff.wgsl:79-128 with per-ray terms amortised): 34 FP32 FMA-pipe
+# operations and 4 SFU operations (rsqrt, rcp, sin, cos).
+FMA_OPS_PER_PAIR = 34
+SFU_OPS_PER_PAIR = 4
+FMA_LANES_PER_SM = 128
+SFU_LANES_PER_SM = 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--rays", type=int, default=1 << 20)
+    ap.add_argument("--grid", type=int, default=512)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smmax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smmax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smmax)) if smmax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(rays, screen, seconds: float):
+    """The oracle on a bounded sample of screen points, all host threads."""
+    from oracle import oracle  # checker / baseline only
+    from xrt_rs import synth
+
+    rl = [rays[k] for k in ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re",
+                            "ep_im", "energy")]
+    threads = oracle.max_threads()
+    count = 8
+    rate = None
+    while True:
+        sub, _ = synth.subsample_screen(screen, count, seed=7)
+        t0 = time.perf_counter()
+        oracle.kahan_f64(rl, [sub["x"], sub["y"], sub["z"]])
+        dt = time.perf_counter() - t0
+        rate = len(rl[0]) * count / dt
+        if dt >= seconds * 0.5 or count >= len(screen["x"]):
+            break
+        count = int(min(len(screen["x"]), max(count * 2, count * seconds * 0.6 / max(dt, 1e-3))))
+    return {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(rl[0])} rays x {count} seeded screen points of the workload "
+                      f"({dt:.1f} s, C restatement of src/waves/diffraction.rs:56-117, "
+                      f"OpenMP over screen points)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    from xrt_rs import synth
+
+    rays, screen = synth.config1(seed=0, n_rays=args.rays, grid=args.grid)
+    rl = [rays[k] for k in ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re",
+                            "ep_im", "energy")]
+    threads = oracle.max_threads()
+    # Size one step to ~2 s of CPU work.
+    sub, _ = synth.subsample_screen(screen, 16, seed=7)
+    t0 = time.perf_counter()
+    oracle.kahan_f64(rl, [sub["x"], sub["y"], sub["z"]])
+    per_point = (time.perf_counter() - t0) / 16
+    count = int(max(16, min(len(screen["x"]), 2.0 / max(per_point, 1e-6))))
+    sub, _ = synth.subsample_screen(screen, count, seed=7)
+    pl = [sub["x"], sub["y"], sub["z"]]
+    for _ in range(args.warmup):
+        oracle.kahan_f64(rl, pl)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.kahan_f64(rl, pl)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.mean(times))
+    pairs = len(rl[0]) * count
+    value = pairs / (ms / 1e3) / 1e9
+    sample = (f"{len(rl[0])} rays x {count} seeded screen points of the 512x512 grid per step; "
+              f"C restatement of src/waves/diffraction.rs:56-117 (the Rust reference cannot be "
+              f"built: no cargo), OpenMP over screen points")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"single solve, {args.rays} rays x {args.grid}x{args.grid} screen "
+                               "(CPU sample)", "rays": args.rays, "screen": args.grid ** 2},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import xrt_rs
+    from xrt_rs import synth
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", local if world > 1 else 0)
+    ctx = xrt_rs.GpuContext.new(dev.index)
+    if ctx is None:
+        raise RuntimeError("no CUDA device")
+
+    rays, screen = synth.config1(seed=rank, n_rays=args.rays, grid=args.grid)
+    fields = xrt_rs.RAY_FIELDS
+    d_rays = [torch.from_numpy(rays[k]).to(dev) for k in fields]
+    d_pix = [torch.from_numpy(screen[k]).to(dev) for k in "xyz"]
+    m = len(screen["x"])
+    n = len(rays["x"])
+    d_out = [torch.zeros(m, dtype=torch.float64, device=dev) for _ in range(4)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    pairs = float(n) * float(m)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def solve(path):
+        return xrt_rs.diffraction_integral_device(d_rays, d_pix, d_out, path=path, ctx=ctx,
+                                                  stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        solve("f32pr")
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(dev.index)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms, kern_ms, launches = [], [], 0
+    stats = None
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        stats = solve("f32pr")
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        kern_ms.append(stats["main_kernel_ms"])
+        launches += stats["kernels"]
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = float(np.mean(step_ms))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = pairs * world / (ms / 1e3) / 1e9
+    out32 = [t.cpu().numpy() for t in d_out]
+
+    # End to end through the host C ABI: pinned host inputs -> field on host.
+    e2e = None
+    if not args.no_e2e:
+        h_rays = [torch.from_numpy(rays[k]).pin_memory().numpy() for k in fields]
+        h_pix = [torch.from_numpy(screen[k]).pin_memory().numpy() for k in "xyz"]
+        xrt_rs.diffraction_integral(h_rays, h_pix, path="f32pr", ctx=ctx)
+        times = []
+        st = None
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, st = xrt_rs.diffraction_integral(h_rays, h_pix, path="f32pr", ctx=ctx,
+                                                return_stats=True)
+            times.append(time.perf_counter() - t0)
+        e2e_ms = 1e3 * float(np.mean(times))
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": pairs * world / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
+               "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(st["h2d_bytes"]),
+               "d2h_bytes_per_step": int(st["d2h_bytes"])}
+
+    # The plain FP64 form on the same inputs, and the FP32 form's error vs it.
+    fp64 = None
+    if not args.no_fp64:
+        solve("f64")
+        torch.cuda.synchronize()
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st64 = solve("f64")
+        e1.record(stream)
+        e1.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        out64 = [t.cpu().numpy() for t in d_out]
+        a = np.concatenate([out32[0] + 1j * out32[1], out32[2] + 1j * out32[3]])
+        b = np.concatenate([out64[0] + 1j * out64[1], out64[2] + 1j * out64[3]])
+        ia = np.abs(a[:m]) ** 2 + np.abs(a[m:]) ** 2
+        ib = np.abs(b[:m]) ** 2 + np.abs(b[m:]) ** 2
+        fp64 = {"value": pairs / (ms64 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms64,
+                "speedup_f32pr_vs_f64": (pairs / (ms / 1e3)) / (pairs / (ms64 / 1e3)),
+                "rel_l2_field_f32pr_vs_f64": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                "rel_l2_intensity_f32pr_vs_f64": float(np.linalg.norm(ia - ib) / np.linalg.norm(ib))}
+
+    # Roofline of the pair kernel: FP32-FMA / SFU pair rate at the sampled clock.
+    props = torch.cuda.get_device_properties(dev)
+    sms = props.multi_processor_count
+    clk_mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    pair_per_clk_sm = min(FMA_LANES_PER_SM / FMA_OPS_PER_PAIR, SFU_LANES_PER_SM / SFU_OPS_PER_PAIR)
+    peak = sms * pair_per_clk_sm * clk_mhz * 1e6 / 1e9
+    kms = float(np.mean(kern_ms))
+    achieved = pairs / (kms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "pr_persistent_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch_full_size")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "fp32_sfu", "achieved": achieved, "peak": peak, "unit": UNIT,
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "pr_persistent_kernel", "kernel_ms": kms,
+                "peak_source": (f"{sms} SMs x min(128 FP32 lanes / {FMA_OPS_PER_PAIR} FMA-pipe ops, "
+                                f"16 SFU lanes / {SFU_OPS_PER_PAIR} SFU ops) per pair x "
+                                f"{clk_mhz:.0f} MHz median SM clock sampled in the timed region"),
+                "algorithmic_ops_per_pair": {"fma_pipe": FMA_OPS_PER_PAIR, "sfu": SFU_OPS_PER_PAIR}}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(rays, screen, args.cpu_seconds)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"single solve: {n} rays (Gaussian aperture sigma 0.1 mm, 10 keV) x "
+                               f"{args.grid}x{args.grid} screen +-0.5 mm at 1000 mm",
+                   "rays": n, "screen_points": m, "pairs_per_step": pairs,
+                   "parallelism": f"replica x{world}", "l2": "flushed between steps (256 MiB write)",
+                   "path": "f32pr", "phase_bound_rad": stats["phase_bound_rad"],
+                   "n_tiles": stats["n_tiles"], "n_chunks": stats["n_chunks"],
+                   "groups": stats["groups"]},
+        "e2e": e2e, "fp64_plain": fp64, "roofline": roofline, "cpu_baseline": cpu,
+        "clocks": clk, "gpu_launches": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

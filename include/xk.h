@@ -1,0 +1,176 @@
+/*
+ * xk — B200-native Kirchhoff diffraction engine, C ABI.
+ *
+ * Drop-in boundary for the Kirchhoff path of physwkim/xrt-rs. Every entry
+ * point takes plain pointers and sizes; nothing in these signatures is a
+ * torch or CUDA-runtime type (streams are passed as `void*`, i.e. a
+ * cudaStream_t or NULL for the library's own stream).
+ *
+ * Units and conventions follow the reference: positions in mm, energies in
+ * eV, k = E / CHBAR * 1e7 mm^-1 with CHBAR = 1973.2697177417986 eV*A
+ * (src/core/consts.rs:74). For every screen point p the library returns
+ *   Es(p) = sum_j es_j * U_j(p),  Ep(p) = sum_j ep_j * U_j(p),
+ *   U_j(p) = i*k_j/(4*pi) * (nl_j + n_j.(p - r_j)/|p - r_j|) * exp(i*k_j*|p - r_j|) / |p - r_j|,
+ * skipping rays with |p - r_j| < 1e-30 (src/waves/diffraction.rs:67-117).
+ *
+ * Two compute paths:
+ *   XK_PATH_F64    the reference algorithm run directly in FP64 on the GPU,
+ *                  per-pixel complex Kahan summation (the parity path).
+ *   XK_PATH_F32PR  FP32 phase-reduced form: per (screen tile, ray chunk)
+ *                  item the phase is split into FP64 per-pixel and per-ray
+ *                  parts and an FP32 residual, compensated two-float
+ *                  accumulation, FP64 cross-chunk reduction. Solves it cannot
+ *                  bound (mixed energies within a chunk, rays touching the
+ *                  screen) are routed to XK_PATH_F64 and reported in stats.
+ *
+ * Every call blocks until its results are in the caller's buffers, like the
+ * reference's pollster::block_on (src/gpu/kirchhoff.rs:82). Calls on one
+ * context are serialised by a mutex; use one context per thread for
+ * concurrency, or the server API for continuous batching.
+ *
+ * There is no CPU fallback: without a CUDA device every compute entry point
+ * returns XK_ERR_NO_DEVICE.
+ */
+#ifndef XK_H
+#define XK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    XK_OK = 0,
+    XK_ERR_NO_DEVICE = 1, /* no usable CUDA device */
+    XK_ERR_INVALID = 2,   /* null pointer, length mismatch, size out of range */
+    XK_ERR_OOM = 3,       /* device or pinned-host allocation failed */
+    XK_ERR_BUDGET = 4,    /* request larger than the configured HBM budget */
+    XK_ERR_CUDA = 5,      /* CUDA runtime or kernel error */
+    XK_ERR_TIMEOUT = 6,   /* a bounded wait ran out */
+    XK_ERR_NOT_FOUND = 7, /* unknown handle or ticket */
+    XK_ERR_CANCELLED = 8, /* request cancelled before completion */
+    XK_ERR_SHUTDOWN = 9   /* server is shutting down */
+};
+
+enum { XK_PATH_F64 = 0, XK_PATH_F32PR = 1 };
+
+/* ---- data structures --------------------------------------------------- */
+
+/* Rays on the optical element, structure of arrays, one f64 per ray in each
+ * array. Field meaning follows DiffractionRay (src/waves/diffraction.rs:16-33)
+ * and the argument order of diffraction_integral_rs
+ * (crates/xrt-python/src/lib.rs:323-339). */
+typedef struct xk_rays {
+    const double *x, *y, *z;     /* position [mm] */
+    const double *nx, *ny, *nz;  /* surface normal */
+    const double *nl;            /* obliquity factor n.l */
+    const double *es_re, *es_im; /* s-polarised amplitude */
+    const double *ep_re, *ep_im; /* p-polarised amplitude */
+    const double *energy;        /* [eV] */
+} xk_rays;
+
+/* Screen points (PixelPoint, src/waves/diffraction.rs:36-41). */
+typedef struct xk_pixels {
+    const double *x, *y, *z;
+} xk_pixels;
+
+/* Output field per screen point (DiffractionResult, diffraction.rs:44-48). */
+typedef struct xk_field {
+    double *es_re, *es_im, *ep_re, *ep_im;
+} xk_field;
+
+/* GpuRay, 48 bytes, f32 (src/gpu/kirchhoff.rs:20-35). */
+typedef struct xk_gpu_ray {
+    float x, y, z, nx, ny, nz, nl, energy, es_re, es_im, ep_re, ep_im;
+} xk_gpu_ray;
+
+/* GpuPixel, 16 bytes (src/gpu/kirchhoff.rs:38-45). */
+typedef struct xk_gpu_pixel {
+    float x, y, z, _pad;
+} xk_gpu_pixel;
+
+/* Per-call report. */
+typedef struct xk_stats {
+    double pairs;            /* n_rays * n_pix */
+    double gpu_ms;           /* device time of the compute kernels (CUDA events) */
+    double wall_ms;          /* host wall time of the whole call incl. copies */
+    int path;                /* XK_PATH_* actually used */
+    int kernels;             /* kernel launches issued by the call */
+    int n_tiles;             /* screen tiles (F32PR) */
+    int n_chunks;            /* ray chunks (F32PR) */
+    long long n_items;       /* work items (F32PR) */
+    double phase_bound_rad;  /* planner's bound on the FP32 residual phase */
+    double h2d_bytes, d2h_bytes;
+    double main_kernel_ms;   /* device time of the pair kernel alone (CUDA events) */
+    int groups;              /* ray groups per tile (F32PR) */
+    int routed_reason;       /* 0 = not routed; see xk_route_reason() */
+} xk_stats;
+
+/* ---- context ------------------------------------------------------------ */
+typedef struct xk_ctx xk_ctx;
+
+/* GpuContext::new (src/gpu/context.rs:20-22,33-67): create a context on CUDA
+ * device `device`. Returns XK_ERR_NO_DEVICE when there is none. */
+int xk_init(int device, xk_ctx** out);
+
+/* GpuContext::shared (src/gpu/context.rs:28-31): the process-wide context on
+ * device 0, created at most once. *out is NULL when no device exists. */
+int xk_shared(xk_ctx** out);
+
+/* Frees a context made by xk_init (the shared one is never freed). */
+void xk_destroy(xk_ctx* ctx);
+
+/* GpuContext::adapter_name (src/gpu/context.rs:70-72). */
+const char* xk_device_name(const xk_ctx* ctx);
+
+/* Message of the last failure on this context ("" if none). */
+const char* xk_last_error(const xk_ctx* ctx);
+
+/* Static description of a status code. */
+const char* xk_status_string(int status);
+
+/* Library version string. */
+const char* xk_version(void);
+
+/* Why an XK_PATH_F32PR request ran on XK_PATH_F64 (xk_stats.routed_reason). */
+const char* xk_route_reason(int reason);
+
+/* ---- single solves --------------------------------------------------------- */
+
+/* waves::diffraction::diffraction_integral (src/waves/diffraction.rs:56-64)
+ * and the PyO3 wrapper diffraction_integral_rs
+ * (crates/xrt-python/src/lib.rs:321-393). Host buffers in, host buffers out.
+ * `path` is XK_PATH_F64 (parity with the reference) or XK_PATH_F32PR.
+ * n_rays == 0 yields zeros; n_pix == 0 is a no-op. `stats` may be NULL. */
+int xk_diffraction_integral(xk_ctx* ctx, const xk_rays* rays, size_t n_rays,
+                            const xk_pixels* pixels, size_t n_pix, xk_field* out,
+                            int path, xk_stats* stats);
+
+/* Same with every pointer in rays/pixels/out a DEVICE pointer, launched on
+ * `stream` (cudaStream_t, NULL = the context's stream). Returns after the
+ * results are written and the stream is synchronised. */
+int xk_diffraction_integral_device(xk_ctx* ctx, const xk_rays* rays, size_t n_rays,
+                                   const xk_pixels* pixels, size_t n_pix, xk_field* out,
+                                   int path, void* stream, xk_stats* stats);
+
+/* gpu::kirchhoff::kirchhoff_gpu (src/gpu/kirchhoff.rs:77-83): GpuRay /
+ * GpuPixel records in, (Es, Ep) per pixel out as 4 doubles per pixel
+ * (es.re, es.im, ep.re, ep.im) — the memory layout of
+ * Vec<(Complex64, Complex64)>. Runs XK_PATH_F32PR with the base phase
+ * restored in FP64. */
+int xk_kirchhoff_gpu(xk_ctx* ctx, const xk_gpu_ray* rays, size_t n_rays,
+                     const xk_gpu_pixel* pixels, size_t n_pix, double* out);
+
+/* gpu::fallback::kirchhoff_auto (src/gpu/fallback.rs:19-26) on the shared
+ * context. Unlike the reference there is no CPU fallback: with no device it
+ * returns XK_ERR_NO_DEVICE. */
+int xk_kirchhoff_auto(const xk_gpu_ray* rays, size_t n_rays, const xk_gpu_pixel* pixels,
+                      size_t n_pix, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XK_H */

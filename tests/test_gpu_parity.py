@@ -1,0 +1,190 @@
+"""GPU parity: libxk.so against the CPU oracle on the same seeded inputs.
+
+Tolerances:
+  XK_PATH_F64   rel L2 <= 1e-10 on the complex field (and abs 1e-10 per
+                component on the reference fixture);
+  XK_PATH_F32PR rel L2 <= 1e-4 on the complex field and on |E|^2.
+"""
+import numpy as np
+import pytest
+
+import cases
+import xrt_rs
+from xrt_rs import synth
+
+pytestmark = pytest.mark.gpu
+
+F64_TOL = 1e-10
+PR_TOL = 1e-4
+COMPS = ("es_re", "es_im", "ep_re", "ep_im")
+
+
+def run(ctx, rays, pix, path):
+    r, p = cases.as_lists(rays, pix)
+    out, st = xrt_rs.diffraction_integral(r, p, path=path, ctx=ctx, return_stats=True)
+    return out, st
+
+
+def oracle_run(oracle, rays, pix):
+    return oracle.kahan_f64(*cases.as_lists(rays, pix))
+
+
+def test_fixture_f64_abs_1e10(ctx, golden_case):
+    rays = [golden_case["rays"][k] for k in cases.RAY_FIELDS]
+    pix = [golden_case["pixels"][k] for k in cases.PIXEL_FIELDS]
+    out = xrt_rs.diffraction_integral_rs(*rays, *pix)
+    for i, exp in enumerate(golden_case["expected"]):
+        for c, name in enumerate(COMPS):
+            assert abs(out[c][i] - exp[name]) < 1e-10, (i, name)
+
+
+def test_fixture_f32pr(ctx, golden_case):
+    rays = [golden_case["rays"][k] for k in cases.RAY_FIELDS]
+    pix = [golden_case["pixels"][k] for k in cases.PIXEL_FIELDS]
+    out = xrt_rs.diffraction_integral_rs(*rays, *pix, path="f32pr")
+    exp = [np.array([e[c] for e in golden_case["expected"]]) for c in COMPS]
+    assert cases.rel_l2(out, exp) < PR_TOL
+
+
+@pytest.mark.parametrize("builder", [
+    cases.single_ray_single_pixel, cases.parallel_pixels, cases.ray_at_pixel,
+    cases.kahan_stability, cases.polychromatic, cases.symmetry, cases.gpu_short_distance,
+    cases.gpu_extreme_distance])
+def test_reference_unit_cases_f64(ctx, oracle, builder):
+    rays, pix = builder()
+    out, st = run(ctx, rays, pix, "f64")
+    ref = oracle_run(oracle, rays, pix)
+    if np.linalg.norm(np.concatenate(cases.field_c(ref))) == 0:
+        assert np.all(np.concatenate(out) == 0)
+    else:
+        assert cases.rel_l2(out, ref) < F64_TOL
+
+
+@pytest.mark.parametrize("builder", [
+    cases.single_ray_single_pixel, cases.parallel_pixels, cases.kahan_stability,
+    cases.large_ray_count, cases.symmetry, cases.gpu_extreme_distance])
+def test_reference_unit_cases_f32pr(ctx, oracle, builder):
+    rays, pix = builder()
+    out, st = run(ctx, rays, pix, "f32pr")
+    ref = oracle_run(oracle, rays, pix)
+    assert cases.rel_l2(out, ref) < PR_TOL, st
+
+
+def test_polychromatic_routes_to_f64(ctx, oracle):
+    rays, pix = cases.polychromatic()
+    out, st = run(ctx, rays, pix, "f32pr")
+    assert st["path"] == xrt_rs.XK_PATH_F64
+    assert cases.rel_l2(out, oracle_run(oracle, rays, pix)) < F64_TOL
+
+
+def test_coincident_ray_routes_to_f64_and_is_skipped(ctx):
+    rays, pix = cases.ray_at_pixel()
+    out, st = run(ctx, rays, pix, "f32pr")
+    assert st["path"] == xrt_rs.XK_PATH_F64
+    assert all(o[0] == 0.0 for o in out)
+
+
+@pytest.mark.parametrize("n_rays,n_pix", cases.BENCH_SIZES)
+def test_bench_sizes(ctx, oracle, n_rays, n_pix):
+    rays, pix = cases.bench_case(n_rays, n_pix)
+    ref = oracle_run(oracle, rays, pix)
+    out64, _ = run(ctx, rays, pix, "f64")
+    assert cases.rel_l2(out64, ref) < F64_TOL
+    out32, _ = run(ctx, rays, pix, "f32pr")
+    assert cases.rel_l2(out32, ref) < PR_TOL
+
+
+@pytest.mark.parametrize("n_rays", [1, 2, 3, 7, 33, 65, 129])
+@pytest.mark.parametrize("n_pix", [1, 5, 9, 31, 257])
+def test_odd_sizes(ctx, oracle, n_rays, n_pix):
+    rays, pix = cases.random_case(n_rays, n_pix, seed=n_rays * 1000 + n_pix)
+    ref = oracle_run(oracle, rays, pix)
+    out64, _ = run(ctx, rays, pix, "f64")
+    assert cases.rel_l2(out64, ref) < F64_TOL
+    out32, _ = run(ctx, rays, pix, "f32pr")
+    assert cases.rel_l2(out32, ref) < PR_TOL
+
+
+def test_general_normals(ctx, oracle):
+    rays, pix = cases.random_case(3000, 700, seed=11, general_normals=True)
+    ref = oracle_run(oracle, rays, pix)
+    out64, _ = run(ctx, rays, pix, "f64")
+    assert cases.rel_l2(out64, ref) < F64_TOL
+    out32, _ = run(ctx, rays, pix, "f32pr")
+    assert cases.rel_l2(out32, ref) < PR_TOL
+
+
+def test_empty_inputs(ctx):
+    out, _ = run(ctx, cases.rays_from([]), cases.pixels_from([0.0, 1.0], 0.0, 1000.0), "f64")
+    assert all(np.all(o == 0) for o in out)
+    out, _ = run(ctx, cases.rays_from([]), cases.pixels_from([0.0, 1.0], 0.0, 1000.0), "f32pr")
+    assert all(np.all(o == 0) for o in out)
+    out, _ = run(ctx, cases.rays_from([0.0]), cases.pixels_from([], 0.0, 1000.0), "f32pr")
+    assert all(len(o) == 0 for o in out)
+
+
+def test_config0_full(ctx, oracle):
+    rays, pix = synth.config0(seed=0)
+    ref = oracle_run(oracle, rays, pix)
+    out64, _ = run(ctx, rays, pix, "f64")
+    assert cases.rel_l2(out64, ref) < F64_TOL
+    out32, st = run(ctx, rays, pix, "f32pr")
+    assert st["path"] == xrt_rs.XK_PATH_F32PR
+    assert cases.rel_l2(out32, ref) < PR_TOL
+    assert cases.rel_l2_intensity(out32, ref) < PR_TOL
+
+
+def test_deterministic(ctx):
+    rays, pix = synth.config0(seed=1)
+    a, _ = run(ctx, rays, pix, "f32pr")
+    b, _ = run(ctx, rays, pix, "f32pr")
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    a, _ = run(ctx, rays, pix, "f64")
+    b, _ = run(ctx, rays, pix, "f64")
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_config1_subsample_f64_vs_oracle(ctx, oracle):
+    """2^20 rays; 128 seeded screen points of the 512x512 grid."""
+    rays, screen = synth.config1(seed=0)
+    sub, _ = synth.subsample_screen(screen, 128, seed=5)
+    ref = oracle_run(oracle, rays, sub)
+    out64, _ = run(ctx, rays, sub, "f64")
+    assert cases.rel_l2(out64, ref) < F64_TOL
+
+
+def test_config1_full_f32pr_vs_f64(ctx):
+    """Full 512x512 field: F32PR against the GPU F64 path (itself pinned to the
+    oracle by the subsample test above)."""
+    rays, screen = synth.config1(seed=0)
+    ref, st64 = run(ctx, rays, screen, "f64")
+    out, st = run(ctx, rays, screen, "f32pr")
+    assert st["path"] == xrt_rs.XK_PATH_F32PR
+    err = cases.rel_l2(out, ref)
+    err_i = cases.rel_l2_intensity(out, ref)
+    print(f"config1 rel_l2 field={err:.3e} intensity={err_i:.3e} "
+          f"f64 {st64['gpu_ms']:.1f} ms, f32pr {st['gpu_ms']:.1f} ms, stats={st}")
+    assert err < PR_TOL
+    assert err_i < PR_TOL
+
+
+def test_kirchhoff_gpu_records(ctx, oracle, golden_case):
+    """gpu::kirchhoff::kirchhoff_gpu on the fixture (golden_gpu_kirchhoff.rs:103-182)."""
+    r = golden_case["rays"]
+    recs = np.zeros(5, dtype=xrt_rs.GPU_RAY_DTYPE)
+    for k in xrt_rs.GPU_RAY_DTYPE.names:
+        recs[k] = r[k]
+    pix = np.zeros(3, dtype=xrt_rs.GPU_PIXEL_DTYPE)
+    for k in "xyz":
+        pix[k] = golden_case["pixels"][k]
+    es, ep = xrt_rs.kirchhoff_gpu(ctx, recs, pix)
+    es2, ep2 = xrt_rs.kirchhoff_auto(recs, pix)
+    f32 = [recs[k].astype(np.float64) for k in cases.RAY_FIELDS]
+    ref = oracle.plain_f64(f32, [pix[k].astype(np.float64) for k in "xyz"])
+    for i in range(3):
+        c = ref[0][i] + 1j * ref[1][i]
+        assert abs(es[i]) > 1e-10
+        assert abs(es[i] - c) / abs(c) < 1e-4
+        assert abs(es2[i] - c) / abs(c) < 1e-4

@@ -1,0 +1,342 @@
+// C-ABI entry points of the xk library (declared in include/xk.h).
+//
+// The context mirrors gpu::context::GpuContext (src/gpu/context.rs): one per
+// device, a process-wide shared instance, the device name. Calls that take
+// host buffers stage them through device buffers the context keeps and
+// grows, so repeated calls of the same size allocate nothing.
+
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "xk_internal.cuh"
+#include "xk_pr.cuh"
+
+struct xk_ctx {
+    int device = 0;
+    int num_sms = 0;
+    bool is_shared = false;
+    std::string name;
+    std::string last_error;
+    std::mutex mu;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    xk::F64Workspace f64ws;
+    xk::PrWorkspace prws;
+    xk::DevBuf in_rays, in_pix, out_field;
+};
+
+namespace {
+
+const char* kVersion = "xk 0.1.0 (sm_100a)";
+
+int fail(xk_ctx* ctx, const xk::Status& st) {
+    if (ctx) ctx->last_error = st.msg;
+    return st.code;
+}
+
+int fail(xk_ctx* ctx, int code, const char* msg) {
+    if (ctx) ctx->last_error = msg;
+    return code;
+}
+
+xk::Status create_ctx(int device, xk_ctx** out) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();  // clear the sticky "no device" state
+        return xk::Status::Err(XK_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count)
+        return xk::Status::Err(XK_ERR_INVALID, "device index out of range");
+    XK_CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    XK_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    xk_ctx* ctx = new xk_ctx();
+    ctx->device = device;
+    ctx->num_sms = prop.multiProcessorCount;
+    ctx->name = prop.name;
+    cudaError_t e1 = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    cudaError_t e2 = cudaEventCreate(&ctx->ev0);
+    cudaError_t e3 = cudaEventCreate(&ctx->ev1);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+        delete ctx;
+        return xk::Status::Err(XK_ERR_CUDA, "stream/event creation failed");
+    }
+    *out = ctx;
+    return xk::Status::Ok();
+}
+
+void destroy_ctx(xk_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->f64ws.rays.release();
+    ctx->f64ws.partials.release();
+    ctx->prws.release();
+    ctx->in_rays.release();
+    ctx->in_pix.release();
+    ctx->out_field.release();
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+bool rays_ok(const xk_rays* r) {
+    return r && r->x && r->y && r->z && r->nx && r->ny && r->nz && r->nl && r->es_re &&
+           r->es_im && r->ep_re && r->ep_im && r->energy;
+}
+bool pix_ok(const xk_pixels* p) { return p && p->x && p->y && p->z; }
+bool field_ok(const xk_field* f) { return f && f->es_re && f->es_im && f->ep_re && f->ep_im; }
+
+xk::RaysDev to_dev(const xk_rays* r) {
+    return xk::RaysDev{r->x, r->y, r->z, r->nx, r->ny, r->nz, r->nl,
+                       r->es_re, r->es_im, r->ep_re, r->ep_im, r->energy};
+}
+
+// Enqueue one solve on device data; records events around the compute.
+xk::Status enqueue_solve(xk_ctx* ctx, const xk::RaysDev& rays, size_t n_rays,
+                         const xk::PixDev& pix, size_t n_pix, const xk::FieldDev& out, int path,
+                         cudaStream_t stream, xk_stats* stats, int* used_path) {
+    xk::LaunchReport rep;
+    XK_CUDA_TRY(cudaEventRecord(ctx->ev0, stream));
+    int used = path;
+    if (path == XK_PATH_F32PR) {
+        xk::PrReport prep;
+        XK_TRY(xk::pr_solve_enqueue(rays, n_rays, pix, n_pix, out, ctx->prws, stream,
+                                    ctx->num_sms, &prep));
+        rep.kernels += prep.kernels;
+        if (prep.routed_f64) {
+            used = XK_PATH_F64;
+            XK_TRY(xk::f64_enqueue(rays, n_rays, pix, n_pix, out, ctx->f64ws, stream,
+                                   ctx->num_sms, &rep));
+        }
+        if (stats) {
+            stats->n_tiles = prep.n_tiles;
+            stats->n_chunks = prep.n_chunks;
+            stats->n_items = prep.n_items;
+            stats->phase_bound_rad = prep.phase_bound;
+            stats->groups = prep.groups;
+            stats->routed_reason = prep.routed_f64 ? prep.route_reason : 0;
+            stats->main_kernel_ms = prep.main_kernel_ms;
+        }
+    } else {
+        XK_TRY(xk::f64_enqueue(rays, n_rays, pix, n_pix, out, ctx->f64ws, stream, ctx->num_sms,
+                               &rep));
+    }
+    XK_CUDA_TRY(cudaEventRecord(ctx->ev1, stream));
+    if (stats) stats->kernels += rep.kernels;
+    *used_path = used;
+    return xk::Status::Ok();
+}
+
+xk::Status finish_stats(xk_ctx* ctx, xk_stats* stats, int used_path, size_t n_rays,
+                        size_t n_pix) {
+    if (!stats) return xk::Status::Ok();
+    float ms = 0.f;
+    XK_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    stats->gpu_ms = ms;
+    stats->path = used_path;
+    stats->pairs = (double)n_rays * (double)n_pix;
+    return xk::Status::Ok();
+}
+
+xk::Status solve_host(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_pixels* pixels,
+                      size_t n_pix, xk_field* out, int path, xk_stats* stats) {
+    cudaStream_t s = ctx->stream;
+    const size_t nb = n_rays * sizeof(double), mb = n_pix * sizeof(double);
+    XK_TRY(ctx->in_rays.ensure(12 * nb > 0 ? 12 * nb : 8));
+    XK_TRY(ctx->in_pix.ensure(3 * mb));
+    XK_TRY(ctx->out_field.ensure(4 * mb));
+    double* dr = ctx->in_rays.as<double>();
+    const double* hsrc[12] = {rays->x, rays->y, rays->z, rays->nx, rays->ny, rays->nz,
+                              rays->nl, rays->es_re, rays->es_im, rays->ep_re, rays->ep_im,
+                              rays->energy};
+    for (int i = 0; i < 12 && n_rays; ++i)
+        XK_CUDA_TRY(cudaMemcpyAsync(dr + i * n_rays, hsrc[i], nb, cudaMemcpyHostToDevice, s));
+    double* dp = ctx->in_pix.as<double>();
+    XK_CUDA_TRY(cudaMemcpyAsync(dp, pixels->x, mb, cudaMemcpyHostToDevice, s));
+    XK_CUDA_TRY(cudaMemcpyAsync(dp + n_pix, pixels->y, mb, cudaMemcpyHostToDevice, s));
+    XK_CUDA_TRY(cudaMemcpyAsync(dp + 2 * n_pix, pixels->z, mb, cudaMemcpyHostToDevice, s));
+    xk::RaysDev rd;
+    const double** f = reinterpret_cast<const double**>(&rd);
+    for (int i = 0; i < 12; ++i) f[i] = dr + i * n_rays;
+    xk::PixDev pd{dp, dp + n_pix, dp + 2 * n_pix};
+    double* dout = ctx->out_field.as<double>();
+    xk::FieldDev fd{dout, dout + n_pix, dout + 2 * n_pix, dout + 3 * n_pix};
+    int used = path;
+    XK_TRY(enqueue_solve(ctx, rd, n_rays, pd, n_pix, fd, path, s, stats, &used));
+    double* hdst[4] = {out->es_re, out->es_im, out->ep_re, out->ep_im};
+    for (int i = 0; i < 4; ++i)
+        XK_CUDA_TRY(cudaMemcpyAsync(hdst[i], dout + i * n_pix, mb, cudaMemcpyDeviceToHost, s));
+    XK_CUDA_TRY(cudaStreamSynchronize(s));
+    if (stats) {
+        stats->h2d_bytes = 12.0 * nb + 3.0 * mb;
+        stats->d2h_bytes = 4.0 * mb;
+    }
+    return finish_stats(ctx, stats, used, n_rays, n_pix);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* xk_version(void) { return kVersion; }
+
+const char* xk_route_reason(int reason) {
+    if (reason < 0 || reason >= xk::kRouteReasonCount) return "unknown";
+    return xk::kRouteReasons[reason];
+}
+
+const char* xk_status_string(int status) {
+    switch (status) {
+        case XK_OK: return "ok";
+        case XK_ERR_NO_DEVICE: return "no CUDA device";
+        case XK_ERR_INVALID: return "invalid argument";
+        case XK_ERR_OOM: return "out of memory";
+        case XK_ERR_BUDGET: return "request exceeds the HBM budget";
+        case XK_ERR_CUDA: return "CUDA error";
+        case XK_ERR_TIMEOUT: return "timed out";
+        case XK_ERR_NOT_FOUND: return "unknown handle or ticket";
+        case XK_ERR_CANCELLED: return "cancelled";
+        case XK_ERR_SHUTDOWN: return "server shutting down";
+        default: return "unknown status";
+    }
+}
+
+int xk_init(int device, xk_ctx** out) {
+    if (!out) return XK_ERR_INVALID;
+    *out = nullptr;
+    xk::Status st = create_ctx(device, out);
+    return st.code;
+}
+
+int xk_shared(xk_ctx** out) {
+    static std::once_flag once;
+    static xk_ctx* shared = nullptr;
+    static int shared_status = XK_OK;
+    if (!out) return XK_ERR_INVALID;
+    std::call_once(once, [] {
+        xk_ctx* c = nullptr;
+        xk::Status st = create_ctx(0, &c);
+        shared_status = st.code;
+        if (st.ok()) {
+            c->is_shared = true;
+            shared = c;
+        }
+    });
+    *out = shared;
+    return shared ? XK_OK : shared_status;
+}
+
+void xk_destroy(xk_ctx* ctx) {
+    if (!ctx || ctx->is_shared) return;
+    destroy_ctx(ctx);
+}
+
+const char* xk_device_name(const xk_ctx* ctx) { return ctx ? ctx->name.c_str() : ""; }
+
+const char* xk_last_error(const xk_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int xk_diffraction_integral(xk_ctx* ctx, const xk_rays* rays, size_t n_rays,
+                            const xk_pixels* pixels, size_t n_pix, xk_field* out, int path,
+                            xk_stats* stats) {
+    if (!ctx) return XK_ERR_INVALID;
+    if ((n_rays && !rays_ok(rays)) || (n_pix && (!pix_ok(pixels) || !field_ok(out))))
+        return fail(ctx, XK_ERR_INVALID, "null array pointer");
+    if (path != XK_PATH_F64 && path != XK_PATH_F32PR)
+        return fail(ctx, XK_ERR_INVALID, "unknown path");
+    auto t0 = std::chrono::steady_clock::now();
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (n_pix == 0) return XK_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    xk::Status st = solve_host(ctx, rays, n_rays, pixels, n_pix, out, path, stats);
+    if (!st.ok()) return fail(ctx, st);
+    if (stats)
+        stats->wall_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                .count();
+    return XK_OK;
+}
+
+int xk_diffraction_integral_device(xk_ctx* ctx, const xk_rays* rays, size_t n_rays,
+                                   const xk_pixels* pixels, size_t n_pix, xk_field* out,
+                                   int path, void* stream, xk_stats* stats) {
+    if (!ctx) return XK_ERR_INVALID;
+    if ((n_rays && !rays_ok(rays)) || (n_pix && (!pix_ok(pixels) || !field_ok(out))))
+        return fail(ctx, XK_ERR_INVALID, "null array pointer");
+    if (path != XK_PATH_F64 && path != XK_PATH_F32PR)
+        return fail(ctx, XK_ERR_INVALID, "unknown path");
+    auto t0 = std::chrono::steady_clock::now();
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (n_pix == 0) return XK_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    xk::RaysDev rd{};
+    if (n_rays) rd = to_dev(rays);
+    xk::PixDev pd{pixels->x, pixels->y, pixels->z};
+    xk::FieldDev fd{out->es_re, out->es_im, out->ep_re, out->ep_im};
+    int used = path;
+    xk::Status st = enqueue_solve(ctx, rd, n_rays, pd, n_pix, fd, path, s, stats, &used);
+    if (st.ok()) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = xk::Status::Err(XK_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (st.ok()) st = finish_stats(ctx, stats, used, n_rays, n_pix);
+    if (!st.ok()) return fail(ctx, st);
+    if (stats)
+        stats->wall_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                .count();
+    return XK_OK;
+}
+
+int xk_kirchhoff_gpu(xk_ctx* ctx, const xk_gpu_ray* rays, size_t n_rays,
+                     const xk_gpu_pixel* pixels, size_t n_pix, double* out) {
+    if (!ctx) return XK_ERR_INVALID;
+    if ((n_rays && !rays) || (n_pix && (!pixels || !out)))
+        return fail(ctx, XK_ERR_INVALID, "null pointer");
+    if (n_pix == 0) return XK_OK;
+    // Promote the f32 records to f64 SoA (exact), as the reference's host
+    // side promotes them for the base-phase restore (kirchhoff.rs:96-104).
+    std::vector<double> r(12 * n_rays), p(3 * n_pix), o(4 * n_pix);
+    for (size_t i = 0; i < n_rays; ++i) {
+        const xk_gpu_ray& g = rays[i];
+        const float v[12] = {g.x, g.y, g.z, g.nx, g.ny, g.nz, g.nl, g.es_re, g.es_im, g.ep_re,
+                             g.ep_im, g.energy};
+        for (int f = 0; f < 12; ++f) r[f * n_rays + i] = v[f];
+    }
+    for (size_t i = 0; i < n_pix; ++i) {
+        p[i] = pixels[i].x;
+        p[n_pix + i] = pixels[i].y;
+        p[2 * n_pix + i] = pixels[i].z;
+    }
+    const double* b = r.data();
+    xk_rays xr{b, b + n_rays, b + 2 * n_rays, b + 3 * n_rays, b + 4 * n_rays, b + 5 * n_rays,
+               b + 6 * n_rays, b + 7 * n_rays, b + 8 * n_rays, b + 9 * n_rays, b + 10 * n_rays,
+               b + 11 * n_rays};
+    xk_pixels xp{p.data(), p.data() + n_pix, p.data() + 2 * n_pix};
+    xk_field xf{o.data(), o.data() + n_pix, o.data() + 2 * n_pix, o.data() + 3 * n_pix};
+    int rc = xk_diffraction_integral(ctx, &xr, n_rays, &xp, n_pix, &xf, XK_PATH_F32PR, nullptr);
+    if (rc != XK_OK) return rc;
+    for (size_t i = 0; i < n_pix; ++i) {
+        out[4 * i + 0] = o[i];
+        out[4 * i + 1] = o[n_pix + i];
+        out[4 * i + 2] = o[2 * n_pix + i];
+        out[4 * i + 3] = o[3 * n_pix + i];
+    }
+    return XK_OK;
+}
+
+int xk_kirchhoff_auto(const xk_gpu_ray* rays, size_t n_rays, const xk_gpu_pixel* pixels,
+                      size_t n_pix, double* out) {
+    xk_ctx* ctx = nullptr;
+    int rc = xk_shared(&ctx);
+    if (rc != XK_OK || !ctx) return rc == XK_OK ? XK_ERR_NO_DEVICE : rc;
+    return xk_kirchhoff_gpu(ctx, rays, n_rays, pixels, n_pix, out);
+}
+
+}  // extern "C"

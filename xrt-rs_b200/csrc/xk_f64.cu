@@ -1,0 +1,228 @@
+// Plain FP64 Kirchhoff path: the reference algorithm run directly in FP64.
+//
+// Per pair it evaluates exactly the expression of
+// src/waves/diffraction.rs:76-110 (diffraction_at_pixel), with every
+// multiply, add, divide and square root an explicitly rounded intrinsic so
+// nothing is contracted into an FMA, and CUDA's double sincos for the
+// exp(i*k*path) factor. Each thread accumulates its pixels with per-component
+// complex Kahan summation in ray order, as the reference does.
+//
+// Parallel layout: a CTA owns 128*kF64Ppt screen points; the ray list is cut
+// into `splits` contiguous ranges (grid.y) when there are too few screen
+// points to fill 148 SMs. Each range writes its compensated partial sum; a
+// second kernel adds the partials in range order with Kahan summation.
+// Rays are staged through shared memory kF64Stage at a time so every ray
+// record is read from L2 once per CTA.
+
+#include "xk_internal.cuh"
+
+namespace xk {
+namespace {
+
+constexpr int kF64Threads = 128;
+constexpr int kF64Ppt = 2;      // screen points per thread
+constexpr int kF64Stage = 32;   // rays per shared-memory stage
+constexpr int kRecDoubles = 16; // 128-byte ray record
+
+// Packed ray record: x y z nx ny nz nl es_re es_im ep_re ep_im k kf pad*3.
+struct __align__(16) RayRec64 {
+    double x, y, z, nx, ny, nz, nl, es_re, es_im, ep_re, ep_im, k, kf, pad0, pad1, pad2;
+};
+static_assert(sizeof(RayRec64) == kRecDoubles * 8, "ray record is 128 bytes");
+
+// k = E / CHBAR * 1e7 and k/(4*pi) are pure functions of the ray, so they
+// are hoisted out of the pair loop; both are rounded exactly as the
+// reference rounds them (diffraction.rs:89,97).
+__global__ void f64_pack_kernel(RaysDev r, size_t n, RayRec64* __restrict__ out) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    RayRec64 o;
+    o.x = r.x[i];
+    o.y = r.y[i];
+    o.z = r.z[i];
+    o.nx = r.nx[i];
+    o.ny = r.ny[i];
+    o.nz = r.nz[i];
+    o.nl = r.nl[i];
+    o.es_re = r.es_re[i];
+    o.es_im = r.es_im[i];
+    o.ep_re = r.ep_re[i];
+    o.ep_im = r.ep_im[i];
+    double k = __dmul_rn(__ddiv_rn(r.energy[i], kChbar), 1e7);
+    o.k = k;
+    o.kf = __ddiv_rn(k, 4.0 * kPi);
+    o.pad0 = o.pad1 = o.pad2 = 0.0;
+    out[i] = o;
+}
+
+struct Acc {
+    double s[4];  // es_re es_im ep_re ep_im
+    double c[4];  // Kahan compensators
+};
+
+__device__ __forceinline__ void kahan_add(double& sum, double& comp, double term) {
+    double y = __dsub_rn(term, comp);
+    double t = __dadd_rn(sum, y);
+    comp = __dsub_rn(__dsub_rn(t, sum), y);
+    sum = t;
+}
+
+__device__ __forceinline__ void pair_f64(const RayRec64& r, double px, double py, double pz,
+                                         Acc& a) {
+    double dx = __dsub_rn(px, r.x);
+    double dy = __dsub_rn(py, r.y);
+    double dz = __dsub_rn(pz, r.z);
+    double p2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    double path = __dsqrt_rn(p2);
+    if (path < 1e-30) return;  // diffraction.rs:81
+    double nd = __dadd_rn(__dadd_rn(__dmul_rn(r.nx, dx), __dmul_rn(r.ny, dy)), __dmul_rn(r.nz, dz));
+    double ns = __ddiv_rn(nd, path);
+    double phase = __dmul_rn(r.k, path);
+    double s, c;
+    sincos(phase, &s, &c);
+    double obl = __dadd_rn(r.nl, ns);
+    double af = __ddiv_rn(__dmul_rn(r.kf, obl), path);
+    // u = i*af*exp(i*phase) = (-af*sin, af*cos)  (diffraction.rs:98)
+    double ure = -__dmul_rn(af, s);
+    double uim = __dmul_rn(af, c);
+    double tr = __dsub_rn(__dmul_rn(r.es_re, ure), __dmul_rn(r.es_im, uim));
+    double ti = __dadd_rn(__dmul_rn(r.es_re, uim), __dmul_rn(r.es_im, ure));
+    kahan_add(a.s[0], a.c[0], tr);
+    kahan_add(a.s[1], a.c[1], ti);
+    tr = __dsub_rn(__dmul_rn(r.ep_re, ure), __dmul_rn(r.ep_im, uim));
+    ti = __dadd_rn(__dmul_rn(r.ep_re, uim), __dmul_rn(r.ep_im, ure));
+    kahan_add(a.s[2], a.c[2], tr);
+    kahan_add(a.s[3], a.c[3], ti);
+}
+
+__global__ void __launch_bounds__(kF64Threads)
+f64_pairs_kernel(const RayRec64* __restrict__ rays, size_t n_rays, size_t rays_per_split,
+                 PixDev pix, size_t n_pix, FieldDev out, double* __restrict__ partials) {
+    __shared__ RayRec64 sm[kF64Stage];
+    const size_t split = blockIdx.y;
+    const size_t r_begin = split * rays_per_split;
+    const size_t r_end = min(n_rays, r_begin + rays_per_split);
+
+    double px[kF64Ppt], py[kF64Ppt], pz[kF64Ppt];
+    size_t pidx[kF64Ppt];
+    Acc acc[kF64Ppt];
+#pragma unroll
+    for (int i = 0; i < kF64Ppt; ++i) {
+        size_t p = blockIdx.x * (size_t)(kF64Threads * kF64Ppt) + threadIdx.x + i * kF64Threads;
+        pidx[i] = p;
+        size_t q = p < n_pix ? p : n_pix - 1;
+        px[i] = pix.x[q];
+        py[i] = pix.y[q];
+        pz[i] = pix.z[q];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[i].s[c] = acc[i].c[c] = 0.0;
+    }
+
+    for (size_t r0 = r_begin; r0 < r_end; r0 += kF64Stage) {
+        const int cnt = (int)min((size_t)kF64Stage, r_end - r0);
+        __syncthreads();
+        const double* src = reinterpret_cast<const double*>(rays + r0);
+        double* dst = reinterpret_cast<double*>(sm);
+        for (int t = threadIdx.x; t < cnt * kRecDoubles; t += kF64Threads) dst[t] = src[t];
+        __syncthreads();
+        for (int j = 0; j < cnt; ++j) {
+#pragma unroll
+            for (int i = 0; i < kF64Ppt; ++i) pair_f64(sm[j], px[i], py[i], pz[i], acc[i]);
+        }
+    }
+
+#pragma unroll
+    for (int i = 0; i < kF64Ppt; ++i) {
+        size_t p = pidx[i];
+        if (p >= n_pix) continue;
+        if (partials == nullptr) {
+            out.es_re[p] = acc[i].s[0];
+            out.es_im[p] = acc[i].s[1];
+            out.ep_re[p] = acc[i].s[2];
+            out.ep_im[p] = acc[i].s[3];
+        } else {
+            // The compensated value of a Kahan accumulator is sum - comp.
+            double* base = partials + split * 4 * n_pix;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) base[c * n_pix + p] = __dsub_rn(acc[i].s[c], acc[i].c[c]);
+        }
+    }
+}
+
+// Adds the per-range partials of every screen point in range order.
+__global__ void f64_combine_kernel(const double* __restrict__ partials, int splits, size_t n_pix,
+                                   FieldDev out) {
+    size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (p >= n_pix) return;
+    double s[4] = {0, 0, 0, 0}, c[4] = {0, 0, 0, 0};
+    for (int k = 0; k < splits; ++k) {
+        const double* base = partials + (size_t)k * 4 * n_pix;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) kahan_add(s[j], c[j], base[j * n_pix + p]);
+    }
+    out.es_re[p] = s[0];
+    out.es_im[p] = s[1];
+    out.ep_re[p] = s[2];
+    out.ep_im[p] = s[3];
+}
+
+__global__ void zero_field_kernel(FieldDev out, size_t n_pix) {
+    size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (p >= n_pix) return;
+    out.es_re[p] = 0.0;
+    out.es_im[p] = 0.0;
+    out.ep_re[p] = 0.0;
+    out.ep_im[p] = 0.0;
+}
+
+}  // namespace
+
+Status f64_enqueue(const RaysDev& rays, size_t n_rays, const PixDev& pix, size_t n_pix,
+                   const FieldDev& out, F64Workspace& ws, cudaStream_t stream, int num_sms,
+                   LaunchReport* rep) {
+    if (n_pix == 0) return Status::Ok();
+    if (n_rays == 0) {
+        zero_field_kernel<<<(unsigned)((n_pix + 255) / 256), 256, 0, stream>>>(out, n_pix);
+        XK_CUDA_TRY(cudaGetLastError());
+        if (rep) rep->kernels += 1;
+        return Status::Ok();
+    }
+    XK_TRY(ws.rays.ensure(n_rays * sizeof(RayRec64)));
+    RayRec64* packed = ws.rays.as<RayRec64>();
+    f64_pack_kernel<<<(unsigned)((n_rays + 255) / 256), 256, 0, stream>>>(rays, n_rays, packed);
+    XK_CUDA_TRY(cudaGetLastError());
+
+    const size_t pix_per_cta = (size_t)kF64Threads * kF64Ppt;
+    const size_t pix_ctas = (n_pix + pix_per_cta - 1) / pix_per_cta;
+    // Aim for about 32 CTAs per SM in flight; never split below one stage.
+    const size_t want = (size_t)num_sms * 32;
+    size_t splits = (want + pix_ctas - 1) / pix_ctas;
+    size_t max_splits = (n_rays + kF64Stage - 1) / kF64Stage;
+    if (splits > max_splits) splits = max_splits;
+    if (splits > 65535) splits = 65535;
+    if (splits < 1) splits = 1;
+    size_t rays_per_split = (n_rays + splits - 1) / splits;
+    rays_per_split = (rays_per_split + kF64Stage - 1) / kF64Stage * kF64Stage;
+    splits = (n_rays + rays_per_split - 1) / rays_per_split;
+
+    double* partials = nullptr;
+    if (splits > 1) {
+        XK_TRY(ws.partials.ensure(splits * 4 * n_pix * sizeof(double)));
+        partials = ws.partials.as<double>();
+    }
+    dim3 grid((unsigned)pix_ctas, (unsigned)splits);
+    f64_pairs_kernel<<<grid, kF64Threads, 0, stream>>>(packed, n_rays, rays_per_split, pix, n_pix,
+                                                         out, partials);
+    XK_CUDA_TRY(cudaGetLastError());
+    int kernels = 2;
+    if (splits > 1) {
+        f64_combine_kernel<<<(unsigned)((n_pix + 255) / 256), 256, 0, stream>>>(
+            partials, (int)splits, n_pix, out);
+        XK_CUDA_TRY(cudaGetLastError());
+        kernels += 1;
+    }
+    if (rep) rep->kernels += kernels;
+    return Status::Ok();
+}
+
+}  // namespace xk

@@ -1,0 +1,95 @@
+// Internal declarations shared by the xk CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/xk.h"
+
+namespace xk {
+
+// c*hbar [eV*Angstrom], src/core/consts.rs:74; k = E / CHBAR * 1e7 [1/mm].
+constexpr double kChbar = 1973.2697177417986;
+constexpr double kPi = 3.14159265358979323846;
+
+// Status carrying a message; the API layer copies it into the context.
+struct Status {
+    int code = XK_OK;
+    std::string msg;
+    bool ok() const { return code == XK_OK; }
+    static Status Ok() { return Status{}; }
+    static Status Err(int c, std::string m) { return Status{c, std::move(m)}; }
+};
+
+#define XK_CUDA_TRY(expr)                                                                  \
+    do {                                                                                   \
+        cudaError_t err__ = (expr);                                                        \
+        if (err__ != cudaSuccess) {                                                        \
+            return ::xk::Status::Err(err__ == cudaErrorMemoryAllocation ? XK_ERR_OOM       \
+                                                                        : XK_ERR_CUDA,     \
+                                     std::string(#expr) + ": " + cudaGetErrorString(err__)); \
+        }                                                                                  \
+    } while (0)
+
+#define XK_TRY(expr)                      \
+    do {                                  \
+        ::xk::Status st__ = (expr);       \
+        if (!st__.ok()) return st__;      \
+    } while (0)
+
+// A growable device buffer owned by a context (never shrinks until freed).
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    Status ensure(size_t want) {
+        if (want <= bytes) return Status::Ok();
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        size_t rounded = (want + ((size_t)1 << 20) - 1) & ~(((size_t)1 << 20) - 1);
+        XK_CUDA_TRY(cudaMalloc(&ptr, rounded));
+        bytes = rounded;
+        return Status::Ok();
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Device-pointer views used by the launchers.
+struct RaysDev {
+    const double *x, *y, *z, *nx, *ny, *nz, *nl, *es_re, *es_im, *ep_re, *ep_im, *energy;
+};
+struct PixDev {
+    const double *x, *y, *z;
+};
+struct FieldDev {
+    double *es_re, *es_im, *ep_re, *ep_im;
+};
+
+// Scratch owned by a context for the FP64 plain path.
+struct F64Workspace {
+    DevBuf rays;      // packed ray records
+    DevBuf partials;  // split-ray partial sums
+};
+
+struct LaunchReport {
+    int kernels = 0;
+    float gpu_ms = 0.f;
+};
+
+// FP64 plain path (xk_f64.cu). All pointers are device pointers; the call
+// enqueues on `stream` and does not synchronise.
+Status f64_enqueue(const RaysDev& rays, size_t n_rays, const PixDev& pix, size_t n_pix,
+                   const FieldDev& out, F64Workspace& ws, cudaStream_t stream, int num_sms,
+                   LaunchReport* rep);
+
+}  // namespace xk

@@ -1,0 +1,141 @@
+"""ctypes binding of libxk.so (include/xk.h).
+
+The library is the product: there is no pure-Python or CPU fallback. If
+libxk.so has not been built, importing this module raises ImportError with
+the build command.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG_DIR, "libxk.so")
+
+XK_OK = 0
+XK_ERR_NO_DEVICE = 1
+XK_ERR_INVALID = 2
+XK_ERR_OOM = 3
+XK_ERR_BUDGET = 4
+XK_ERR_CUDA = 5
+XK_ERR_TIMEOUT = 6
+XK_ERR_NOT_FOUND = 7
+XK_ERR_CANCELLED = 8
+XK_ERR_SHUTDOWN = 9
+
+XK_PATH_F64 = 0
+XK_PATH_F32PR = 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class XkRays(ctypes.Structure):
+    _fields_ = [(n, _dp) for n in ("x", "y", "z", "nx", "ny", "nz", "nl",
+                                   "es_re", "es_im", "ep_re", "ep_im", "energy")]
+
+
+class XkPixels(ctypes.Structure):
+    _fields_ = [(n, _dp) for n in ("x", "y", "z")]
+
+
+class XkField(ctypes.Structure):
+    _fields_ = [(n, _dp) for n in ("es_re", "es_im", "ep_re", "ep_im")]
+
+
+class XkGpuRay(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ("x", "y", "z", "nx", "ny", "nz", "nl", "energy",
+                                              "es_re", "es_im", "ep_re", "ep_im")]
+
+
+class XkGpuPixel(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ("x", "y", "z", "_pad")]
+
+
+class XkStats(ctypes.Structure):
+    _fields_ = [
+        ("pairs", ctypes.c_double),
+        ("gpu_ms", ctypes.c_double),
+        ("wall_ms", ctypes.c_double),
+        ("path", ctypes.c_int),
+        ("kernels", ctypes.c_int),
+        ("n_tiles", ctypes.c_int),
+        ("n_chunks", ctypes.c_int),
+        ("n_items", ctypes.c_longlong),
+        ("phase_bound_rad", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_double),
+        ("d2h_bytes", ctypes.c_double),
+        ("main_kernel_ms", ctypes.c_double),
+        ("groups", ctypes.c_int),
+        ("routed_reason", ctypes.c_int),
+    ]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# Every entry point include/xk.h declares, with its ctypes signature.
+_SIGNATURES = {
+    "xk_init": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "xk_shared": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p)]),
+    "xk_destroy": (None, [ctypes.c_void_p]),
+    "xk_device_name": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "xk_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "xk_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "xk_version": (ctypes.c_char_p, []),
+    "xk_route_reason": (ctypes.c_char_p, [ctypes.c_int]),
+    "xk_diffraction_integral": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels),
+        ctypes.c_size_t, ctypes.POINTER(XkField), ctypes.c_int, ctypes.POINTER(XkStats)]),
+    "xk_diffraction_integral_device": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels),
+        ctypes.c_size_t, ctypes.POINTER(XkField), ctypes.c_int, ctypes.c_void_p,
+        ctypes.POINTER(XkStats)]),
+    "xk_kirchhoff_gpu": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.POINTER(XkGpuRay), ctypes.c_size_t, ctypes.POINTER(XkGpuPixel),
+        ctypes.c_size_t, _dp]),
+    "xk_kirchhoff_auto": (ctypes.c_int, [
+        ctypes.POINTER(XkGpuRay), ctypes.c_size_t, ctypes.POINTER(XkGpuPixel), ctypes.c_size_t,
+        _dp]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libxk.so and attach signatures (cached)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python xrt-rs_b200/build.py`")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_names():
+    return sorted(_SIGNATURES)
+
+
+class XkError(RuntimeError):
+    """A non-zero status from the library."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"xk error {code}: {message}")
+        self.code = code
+
+
+def check(code: int, ctx=None):
+    if code == XK_OK:
+        return
+    lib = load()
+    msg = lib.xk_status_string(code).decode()
+    if ctx:
+        detail = lib.xk_last_error(ctx)
+        if detail:
+            msg = f"{msg}: {detail.decode()}"
+    raise XkError(code, msg)
