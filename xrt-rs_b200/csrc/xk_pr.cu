@@ -380,7 +380,7 @@ template <int P, bool UNIFORM>
 struct LaneState {
     float vx[P], vy[P], vz[P], q2[P];
     float nq[P];                // 2 n.q (UNIFORM)
-    float qx[P], qy[P], qz[P];  // 2 q (general normals)
+    float qx[P], qy[P], qz[P];  // q (general normals)
     float acc[P][4];
 };
 
@@ -407,9 +407,10 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
         if (UNIFORM) {
             ls.nq[i] = (float)(2.0 * ((double)sv.unx * qx + (double)sv.uny * qy + (double)sv.unz * qz));
         } else {
-            ls.qx[i] = (float)(2.0 * qx);
-            ls.qy[i] = (float)(2.0 * qy);
-            ls.qz[i] = (float)(2.0 * qz);
+            // The prepared record carries 2n, so 2 n.q = (2n).q.
+            ls.qx[i] = (float)qx;
+            ls.qy[i] = (float)qy;
+            ls.qz[i] = (float)qz;
         }
     }
 }
