@@ -355,7 +355,7 @@ def main():
                    "parallelism": f"replica x{world}", "l2": "flushed between steps (256 MiB write)",
                    "path": "f32pr", "phase_bound_rad": stats["phase_bound_rad"],
                    "n_tiles": stats["n_tiles"], "n_chunks": stats["n_chunks"],
-                   "groups": stats["groups"]},
+                   "groups": stats["groups"], "sweep": ["sfu_rcp", "packed_f32x2"][stats["sweep"]]},
         "e2e": e2e, "fp64_plain": fp64, "roofline": roofline, "cpu_baseline": cpu,
         "clocks": clk, "gpu_launches": launches,
     }

@@ -107,6 +107,7 @@ typedef struct xk_stats {
     double main_kernel_ms;   /* device time of the pair kernel alone (CUDA events) */
     int groups;              /* ray groups per tile (F32PR) */
     int routed_reason;       /* 0 = not routed; see xk_route_reason() */
+    int sweep;               /* F32PR sweep used: 0 SFU reciprocal, 1 packed + series, -1 none */
 } xk_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -137,6 +138,14 @@ const char* xk_version(void);
 
 /* Why an XK_PATH_F32PR request ran on XK_PATH_F64 (xk_stats.routed_reason). */
 const char* xk_route_reason(int reason);
+
+/* Tuning knobs of the F32PR path (no counterpart in the reference, whose
+ * shader has no parameters). Names:
+ *   "phase_budget"   bound on the FP32 residual phase in rad (default 256)
+ *   "sweep"          -1 automatic, 0 SFU reciprocal, 1 packed f32x2 sweep
+ *   "groups"         ray ranges per screen tile, 0 = automatic
+ *   "items_per_warp" target work items per resident warp (automatic groups) */
+int xk_set_option(xk_ctx* ctx, const char* name, double value);
 
 /* ---- single solves --------------------------------------------------------- */
 

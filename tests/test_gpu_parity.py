@@ -188,3 +188,43 @@ def test_kirchhoff_gpu_records(ctx, oracle, golden_case):
         assert abs(es[i]) > 1e-10
         assert abs(es[i] - c) / abs(c) < 1e-4
         assert abs(es2[i] - c) / abs(c) < 1e-4
+
+
+@pytest.fixture
+def sweep_ctx(ctx):
+    yield ctx
+    ctx.set_option("sweep", -1)
+
+
+@pytest.mark.parametrize("sweep", [0, 1])
+def test_both_sweeps_config0(sweep_ctx, oracle, sweep):
+    """The SFU-reciprocal sweep and the packed f32x2 series sweep."""
+    sweep_ctx.set_option("sweep", sweep)
+    rays, pix = synth.config0(seed=3)
+    ref = oracle_run(oracle, rays, pix)
+    out, st = run(sweep_ctx, rays, pix, "f32pr")
+    assert st["sweep"] == sweep
+    assert cases.rel_l2(out, ref) < PR_TOL
+    assert cases.rel_l2_intensity(out, ref) < PR_TOL
+
+
+@pytest.mark.parametrize("sweep", [0, 1])
+def test_both_sweeps_general_normals(sweep_ctx, oracle, sweep):
+    sweep_ctx.set_option("sweep", sweep)
+    rays, pix = cases.random_case(2000, 300, seed=21, general_normals=True)
+    out, st = run(sweep_ctx, rays, pix, "f32pr")
+    assert st["sweep"] == sweep
+    assert cases.rel_l2(out, oracle_run(oracle, rays, pix)) < PR_TOL
+
+
+def test_phase_budget_option(sweep_ctx, oracle):
+    """A tighter residual-phase budget gives finer ray chunks and the same field."""
+    rays, pix = synth.config0(seed=4)
+    ref = oracle_run(oracle, rays, pix)
+    sweep_ctx.set_option("phase_budget", 32.0)
+    try:
+        out, st = run(sweep_ctx, rays, pix, "f32pr")
+    finally:
+        sweep_ctx.set_option("phase_budget", 256.0)
+    assert st["phase_bound_rad"] <= 32.0 + 1e-9
+    assert cases.rel_l2(out, ref) < PR_TOL

@@ -23,6 +23,7 @@ struct xk_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     xk::F64Workspace f64ws;
     xk::PrWorkspace prws;
+    xk::PrOptions pr_opts;
     xk::DevBuf in_rays, in_pix, out_field;
 };
 
@@ -95,37 +96,49 @@ xk::RaysDev to_dev(const xk_rays* r) {
                        r->es_re, r->es_im, r->ep_re, r->ep_im, r->energy};
 }
 
-// Enqueue one solve on device data; records events around the compute.
-xk::Status enqueue_solve(xk_ctx* ctx, const xk::RaysDev& rays, size_t n_rays,
-                         const xk::PixDev& pix, size_t n_pix, const xk::FieldDev& out, int path,
-                         cudaStream_t stream, xk_stats* stats, int* used_path) {
+// Runs one solve on device data; records events around the compute and
+// returns after the stream is synchronised.
+xk::Status run_solve(xk_ctx* ctx, const xk::RaysDev& rays, size_t n_rays, const xk::PixDev& pix,
+                     size_t n_pix, const xk::FieldDev& out, int path, cudaStream_t stream,
+                     xk_stats* stats, int* used_path) {
     xk::LaunchReport rep;
     XK_CUDA_TRY(cudaEventRecord(ctx->ev0, stream));
     int used = path;
     if (path == XK_PATH_F32PR) {
-        xk::PrReport prep;
-        XK_TRY(xk::pr_solve_enqueue(rays, n_rays, pix, n_pix, out, ctx->prws, stream,
-                                    ctx->num_sms, &prep));
-        rep.kernels += prep.kernels;
-        if (prep.routed_f64) {
+        std::vector<xk::PrPlan> plans;
+        xk::PrSolveIn in{rays, n_rays, pix, n_pix, out};
+        int nk = 0;
+        XK_TRY(xk::pr_plan(&in, 1, ctx->prws, stream, ctx->num_sms, ctx->pr_opts, plans, &nk));
+        rep.kernels += nk;
+        xk::PrPlan& P = plans[0];
+        xk::PrExecReport er;
+        if (P.routed) {
             used = XK_PATH_F64;
-            XK_TRY(xk::f64_enqueue(rays, n_rays, pix, n_pix, out, ctx->f64ws, stream,
-                                   ctx->num_sms, &rep));
+            XK_TRY(xk::f64_enqueue(rays, n_rays, pix, n_pix, out, ctx->f64ws, stream, ctx->num_sms,
+                                   &rep));
+        } else {
+            XK_TRY(xk::pr_execute_enqueue(plans, ctx->prws, stream, ctx->num_sms, true, &er));
+            rep.kernels += er.kernels;
         }
+        XK_CUDA_TRY(cudaEventRecord(ctx->ev1, stream));
+        XK_CUDA_TRY(cudaStreamSynchronize(stream));
+        if (!P.routed) XK_TRY(xk::pr_execute_finish(plans, ctx->prws, &er));
         if (stats) {
-            stats->n_tiles = prep.n_tiles;
-            stats->n_chunks = prep.n_chunks;
-            stats->n_items = prep.n_items;
-            stats->phase_bound_rad = prep.phase_bound;
-            stats->groups = prep.groups;
-            stats->routed_reason = prep.routed_f64 ? prep.route_reason : 0;
-            stats->main_kernel_ms = prep.main_kernel_ms;
+            stats->n_tiles = P.n_tiles;
+            stats->n_chunks = P.n_chunks;
+            stats->n_items = (long long)P.n_tiles * P.groups;
+            stats->phase_bound_rad = P.phase_bound;
+            stats->groups = P.groups;
+            stats->routed_reason = P.routed ? P.route_reason : 0;
+            stats->main_kernel_ms = er.main_kernel_ms;
+            stats->sweep = P.routed ? -1 : (P.fast ? 1 : 0);
         }
     } else {
         XK_TRY(xk::f64_enqueue(rays, n_rays, pix, n_pix, out, ctx->f64ws, stream, ctx->num_sms,
                                &rep));
+        XK_CUDA_TRY(cudaEventRecord(ctx->ev1, stream));
+        XK_CUDA_TRY(cudaStreamSynchronize(stream));
     }
-    XK_CUDA_TRY(cudaEventRecord(ctx->ev1, stream));
     if (stats) stats->kernels += rep.kernels;
     *used_path = used;
     return xk::Status::Ok();
@@ -166,7 +179,7 @@ xk::Status solve_host(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_
     double* dout = ctx->out_field.as<double>();
     xk::FieldDev fd{dout, dout + n_pix, dout + 2 * n_pix, dout + 3 * n_pix};
     int used = path;
-    XK_TRY(enqueue_solve(ctx, rd, n_rays, pd, n_pix, fd, path, s, stats, &used));
+    XK_TRY(run_solve(ctx, rd, n_rays, pd, n_pix, fd, path, s, stats, &used));
     double* hdst[4] = {out->es_re, out->es_im, out->ep_re, out->ep_im};
     for (int i = 0; i < 4; ++i)
         XK_CUDA_TRY(cudaMemcpyAsync(hdst[i], dout + i * n_pix, mb, cudaMemcpyDeviceToHost, s));
@@ -239,6 +252,29 @@ const char* xk_device_name(const xk_ctx* ctx) { return ctx ? ctx->name.c_str() :
 
 const char* xk_last_error(const xk_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
+int xk_set_option(xk_ctx* ctx, const char* name, double value) {
+    if (!ctx || !name) return XK_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string n(name);
+    if (n == "phase_budget") {
+        if (!(value > 0.0) || value > 1e5) return fail(ctx, XK_ERR_INVALID, "phase_budget out of range");
+        ctx->pr_opts.phase_budget = value;
+    } else if (n == "sweep") {
+        if (value != -1.0 && value != 0.0 && value != 1.0)
+            return fail(ctx, XK_ERR_INVALID, "sweep must be -1, 0 or 1");
+        ctx->pr_opts.sweep = (int)value;
+    } else if (n == "groups") {
+        if (value < 0.0 || value > 65536.0) return fail(ctx, XK_ERR_INVALID, "groups out of range");
+        ctx->pr_opts.groups = (int)value;
+    } else if (n == "items_per_warp") {
+        if (value < 1.0 || value > 4096.0) return fail(ctx, XK_ERR_INVALID, "items_per_warp out of range");
+        ctx->pr_opts.items_per_warp = (long long)value;
+    } else {
+        return fail(ctx, XK_ERR_INVALID, "unknown option");
+    }
+    return XK_OK;
+}
+
 int xk_diffraction_integral(xk_ctx* ctx, const xk_rays* rays, size_t n_rays,
                             const xk_pixels* pixels, size_t n_pix, xk_field* out, int path,
                             xk_stats* stats) {
@@ -280,11 +316,7 @@ int xk_diffraction_integral_device(xk_ctx* ctx, const xk_rays* rays, size_t n_ra
     xk::PixDev pd{pixels->x, pixels->y, pixels->z};
     xk::FieldDev fd{out->es_re, out->es_im, out->ep_re, out->ep_im};
     int used = path;
-    xk::Status st = enqueue_solve(ctx, rd, n_rays, pd, n_pix, fd, path, s, stats, &used);
-    if (st.ok()) {
-        cudaError_t e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) st = xk::Status::Err(XK_ERR_CUDA, cudaGetErrorString(e));
-    }
+    xk::Status st = run_solve(ctx, rd, n_rays, pd, n_pix, fd, path, s, stats, &used);
     if (st.ok()) st = finish_stats(ctx, stats, used, n_rays, n_pix);
     if (!st.ok()) return fail(ctx, st);
     if (stats)

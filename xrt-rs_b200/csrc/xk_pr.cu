@@ -9,8 +9,8 @@
 // with v = q - |q| u (|v| <= tile radius) and rho_perp = rho - (u.rho) u.
 // The denominator equals 2(|q| - u.rho) + Delta, and Delta/|q| is far below
 // FP32 resolution, so the kernel uses 2(|q| - u.rho).
-//   * exp(i k |q|)      per screen point and chunk, FP64 (reference path
-//                       length and restored base phase),
+//   * exp(i k |q|)      per screen point and chunk: reference path length and
+//                       its turn count in FP64, sin/cos of the reduced turn,
 //   * exp(-i k u.rho)   per ray and item, FP64 argument reduction folded
 //                       into the ray's amplitudes,
 //   * exp(i k Delta)    per pair, FP32: |k Delta| <= phase_budget by
@@ -19,7 +19,7 @@
 // (src/gpu/shaders/kirchhoff.wgsl:95-113, src/gpu/kirchhoff.rs:96-104,
 // 276-297), whose FP32 residual is unbounded at high Fresnel numbers.
 //
-// Work decomposition. Screen points are sorted along a Morton curve and cut
+// Work decomposition. Screen points are sorted along a Hilbert curve and cut
 // into tiles of 32*kPrPpl points (one warp, kPrPpl points per lane). Rays are
 // binned into a grid of cells sized so that the residual phase bound holds
 // for every (tile, cell) pair; each occupied cell is a chunk. The sorted ray
@@ -29,15 +29,22 @@
 // cp.async.bulk (TMA bulk copy, mbarrier completion, two buffers), prepared
 // in place for the item's direction u, and swept by all 32 lanes. Each lane
 // keeps per-point FP32 partial sums folded every stage into two-float
-// (TwoSum) accumulators; at a chunk boundary they are multiplied by the FP64
-// per-point phasor and added to the item's FP64 slot. A final pass adds the
-// `groups` slots of every point in order, so results are deterministic.
+// (TwoSum) accumulators; at a chunk boundary they are multiplied by the
+// per-point phasor and added, in FP64, to the item's slot. A final pass adds
+// the `groups` slots of every point in order, so results are deterministic.
+//
+// Two sweeps: the SFU sweep (rcp.approx for 1/(2|q| - 2u.rho)) and the packed
+// sweep, which processes two screen points per instruction with the sm_100
+// f32x2 FMA and replaces the reciprocal by the series
+// r0 (1 + e + e^2), r0 = 1/(2|q|), e = 2u.rho r0, when the planner can bound
+// |e| (the neglected e^3 term then stays below 1e-8 relative).
 
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "xk_pr.cuh"
@@ -48,6 +55,8 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kSumFields = 26;
 constexpr uint32_t kMaxWaitIters = 1u << 24;
+// |e| bound under which the packed sweep's series reciprocal is used.
+constexpr double kSeriesRcpBound = 2e-3;
 
 // ---------------------------------------------------------------------------
 // Planner kernels
@@ -55,12 +64,14 @@ constexpr uint32_t kMaxWaitIters = 1u << 24;
 
 enum : int { OP_SUM = 0, OP_MIN = 1, OP_MAX = 2 };
 __constant__ int c_sum_ops[kSumFields] = {
-    OP_SUM, OP_SUM, OP_SUM,  // ray position sums
+    OP_SUM, OP_SUM, OP_SUM,                          // ray position sums
     OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX,  // ray bbox
     OP_MIN, OP_MAX,                                  // energy range
     OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX,  // normal range
     OP_SUM, OP_SUM, OP_SUM,                          // screen position sums
     OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX}; // screen bbox
+const int h_sum_ops[kSumFields] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 1, 2, 1, 1,
+                                   1, 2, 2, 2, 0, 0, 0, 1, 1, 1, 2, 2, 2};
 
 __device__ __forceinline__ double op_combine(int op, double a, double b) {
     return op == OP_SUM ? a + b : (op == OP_MIN ? fmin(a, b) : fmax(a, b));
@@ -108,7 +119,7 @@ __global__ void __launch_bounds__(256) summary_kernel(RaysDev r, int n, PixDev p
 struct Frame {
     double ox, oy, oz;  // origin
     double e1[3], e2[3], u0[3];
-    double lo[3], scale[3];  // quantisation: key_a = (coord_a - lo_a) * scale_a
+    double lo[3], scale[3];  // quantisation: q_a = (coord_a - lo_a) * scale_a
 };
 
 __device__ __forceinline__ void to_frame(const Frame& fr, double x, double y, double z,
@@ -119,39 +130,54 @@ __device__ __forceinline__ void to_frame(const Frame& fr, double x, double y, do
     out[2] = dx * fr.u0[0] + dy * fr.u0[1] + dz * fr.u0[2];
 }
 
-__device__ __forceinline__ uint64_t spread21(uint64_t v) {
-    v &= 0x1fffff;
-    v = (v | v << 32) & 0x1f00000000ffffull;
-    v = (v | v << 16) & 0x1f0000ff0000ffull;
-    v = (v | v << 8) & 0x100f00f00f00f00full;
-    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
-    v = (v | v << 2) & 0x1249249249249249ull;
-    return v;
-}
-
-__device__ __forceinline__ uint64_t quant21(double v) {
+__device__ __forceinline__ uint32_t quant(double v, double maxv) {
     double q = floor(v);
-    q = fmin(fmax(q, 0.0), 2097151.0);
-    return (uint64_t)q;
+    q = fmin(fmax(q, 0.0), maxv);
+    return (uint32_t)q;
 }
 
-// Morton key of every screen point in the frame.
+// Distance of (x, y) along the Hilbert curve of order 16 (the classic
+// iterative xy -> d mapping: quadrant digit per level, then rotate/flip).
+__device__ __forceinline__ uint32_t hilbert16(uint32_t x, uint32_t y) {
+    uint32_t d = 0;
+    for (uint32_t s = 1u << 15; s > 0; s >>= 1) {
+        uint32_t rx = (x & s) ? 1u : 0u;
+        uint32_t ry = (y & s) ? 1u : 0u;
+        d += s * s * ((3u * rx) ^ ry);
+        if (ry == 0) {
+            if (rx == 1) {
+                x = 0xffffu - x;
+                y = 0xffffu - y;
+            }
+            uint32_t t = x;
+            x = y;
+            y = t;
+        }
+    }
+    return d;
+}
+
+// Hilbert key of every screen point over its two transverse frame axes, the
+// longitudinal coordinate as tie-break.
 __global__ void pixel_keys_kernel(PixDev p, int m, Frame fr, uint64_t* __restrict__ keys,
                                   int* __restrict__ idx) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     double c[3];
     to_frame(fr, p.x[i], p.y[i], p.z[i], c);
-    uint64_t k = spread21(quant21((c[0] - fr.lo[0]) * fr.scale[0])) |
-                 spread21(quant21((c[1] - fr.lo[1]) * fr.scale[1])) << 1 |
-                 spread21(quant21((c[2] - fr.lo[2]) * fr.scale[2])) << 2;
-    keys[i] = k;
+    uint32_t hx = quant((c[0] - fr.lo[0]) * fr.scale[0], 65535.0);
+    uint32_t hy = quant((c[1] - fr.lo[1]) * fr.scale[1], 65535.0);
+    uint32_t hz = quant((c[2] - fr.lo[2]) * fr.scale[2], 2097151.0);
+    keys[i] = ((uint64_t)hilbert16(hx, hy) << 21) | hz;
     idx[i] = i;
 }
 
-// One warp per tile: slot table, bounding-box centre, radius.
+// One warp per tile: slot table, slot-ordered coordinates, bounding-box
+// centre, radius.
 __global__ void tile_kernel(PixDev p, int m, int n_tiles, const int* __restrict__ sorted_idx,
-                            int* __restrict__ tile_perm, double* __restrict__ tile_center,
+                            int* __restrict__ tile_perm, double* __restrict__ tpx,
+                            double* __restrict__ tpy, double* __restrict__ tpz,
+                            double* __restrict__ tile_center,
                             unsigned long long* __restrict__ amax_bits) {
     int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
@@ -179,10 +205,17 @@ __global__ void tile_kernel(PixDev p, int m, int n_tiles, const int* __restrict_
     for (int i = 0; i < kPrPpl; ++i) {
         long long s = (long long)t * kPrTile + lane + 32 * i;
         int id = s < m ? sorted_idx[s] : -1;
+        double x = c[0], y = c[1], z = c[2];
         if (id >= 0) {
-            double dx = p.x[id] - c[0], dy = p.y[id] - c[1], dz = p.z[id] - c[2];
+            x = p.x[id];
+            y = p.y[id];
+            z = p.z[id];
+            double dx = x - c[0], dy = y - c[1], dz = z - c[2];
             rad = fmax(rad, sqrt(dx * dx + dy * dy + dz * dz));
         }
+        tpx[s] = x;
+        tpy[s] = y;
+        tpz[s] = z;
     }
     for (int o = 16; o > 0; o >>= 1) rad = fmax(rad, __shfl_xor_sync(kFull, rad, o));
     if (lane == 0) {
@@ -194,9 +227,9 @@ __global__ void tile_kernel(PixDev p, int m, int n_tiles, const int* __restrict_
 }
 
 struct CellGrid {
-    Frame fr;                 // origin, axes, lo[] (cell-grid origin in frame coords)
-    double cell[3];           // cell size per axis
-    long long n[3];           // cells per axis
+    Frame fr;        // origin, axes, lo[] (cell-grid origin in frame coords)
+    double cell[3];  // cell size per axis
+    long long n[3];  // cells per axis
 };
 
 __device__ __forceinline__ void cell_of(const CellGrid& g, double x, double y, double z,
@@ -278,20 +311,24 @@ __global__ void records_kernel(RaysDev r, int n, const int* __restrict__ sorted_
     recs[i] = rec;
 }
 
-__global__ void finalize_kernel(const double* __restrict__ partial, int groups, int m,
-                                FieldDev out) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= m) return;
-    double s[4] = {0.0, 0.0, 0.0, 0.0};
+// Adds the groups' slots of every tile slot in order and scatters the sum to
+// the screen point's original index.
+__global__ void finalize_kernel(const double* __restrict__ partial, const int* __restrict__ tile_perm,
+                                int groups, int slots, FieldDev out) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slots) return;
+    int id = tile_perm[s];
+    if (id < 0) return;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int g = 0; g < groups; ++g) {
-        const double* b = partial + (size_t)g * 4 * m;
+        const double* b = partial + (size_t)g * 4 * slots;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) s[c] += b[(size_t)c * m + p];
+        for (int c = 0; c < 4; ++c) acc[c] += b[(size_t)c * slots + s];
     }
-    out.es_re[p] = s[0];
-    out.es_im[p] = s[1];
-    out.ep_re[p] = s[2];
-    out.ep_im[p] = s[3];
+    out.es_re[id] = acc[0];
+    out.es_im[id] = acc[1];
+    out.ep_re[id] = acc[2];
+    out.ep_im[id] = acc[3];
 }
 
 // ---------------------------------------------------------------------------
@@ -360,98 +397,115 @@ __device__ __forceinline__ void two_sum_acc(float& hi, float& lo, float x) {
     lo += err;
 }
 
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
 // Prepared record in shared memory (in place of the 64-byte raw record):
 //   a = {rho_x, rho_y, rho_z, R = k |rho_perp|^2}
-//   b = {W = -2 u.rho, G = -2 n.rho, nl, 0}
+//   b = {W = -2 u.rho, G = -2 n.rho, nl, -W}
 //   e = {es', ep'} with the per-ray phasor exp(-i k u.rho) applied
 //   n = {2 nx, 2 ny, 2 nz, 0}
-
+//
 // Per-warp shared state besides the two ray buffers.
-template <int P>
 struct WarpShared {
-    float hi[P * 4][32];  // two-float accumulators, [point*4 + component][lane]
-    float lo[P * 4][32];
-    double ux, uy, uz;    // item direction for the current chunk
-    double r0x, r0y, r0z; // chunk centre
-    uint64_t bar[2];      // mbarriers of the two ray buffers
+    float hi[kPrPpl * 4][32];  // two-float accumulators, [point*4 + component][lane]
+    float lo[kPrPpl * 4][32];
+    float2 ph[kPrPpl][32];     // (k/2pi) i exp(i k |q|) of the current chunk
+    double ux, uy, uz;         // item direction for the current chunk
+    double r0x, r0y, r0z;      // chunk centre
+    uint64_t bar[2];           // mbarriers of the two ray buffers
 };
 
-template <int P, bool UNIFORM>
-struct LaneState {
-    float vx[P], vy[P], vz[P], q2[P];
-    float nq[P];                // 2 n.q (UNIFORM)
-    float qx[P], qy[P], qz[P];  // q (general normals)
-    float acc[P][4];
+// Per-lane state of the SFU sweep.
+template <bool UNIFORM>
+struct ScalarState {
+    float vx[kPrPpl], vy[kPrPpl], vz[kPrPpl], q2[kPrPpl];  // q2 = 2|q|
+    float nq[kPrPpl];                                        // 2 n.q (UNIFORM)
+    float qx[kPrPpl], qy[kPrPpl], qz[kPrPpl];                // q (general normals)
+    float acc[kPrPpl][4];
 };
 
-template <int P, bool UNIFORM>
-__device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
-                                             const WarpShared<P>& ws, LaneState<P, UNIFORM>& ls) {
-    const double p0x = sv.tile_center[3 * t], p0y = sv.tile_center[3 * t + 1],
-                 p0z = sv.tile_center[3 * t + 2];
+// Per-lane state of the packed sweep: point pairs (2i, 2i+1).
+template <bool UNIFORM>
+struct PackedState {
+    float2 vx[kPrPpl / 2], vy[kPrPpl / 2], vz[kPrPpl / 2], q2[kPrPpl / 2];  // q2 = 1/(2|q|)
+    float2 nq[kPrPpl / 2];
+    float2 qx[kPrPpl / 2], qy[kPrPpl / 2], qz[kPrPpl / 2];
+    float2 acc[kPrPpl / 2][4];
+};
+
+// Per chunk: FP64 geometry of the lane's points, written into the sweep
+// state, and the per-point phasor into shared memory.
+template <bool UNIFORM, bool FAST, class State>
+__device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane, WarpShared& ws,
+                                             State& st) {
     const double ux = ws.ux, uy = ws.uy, uz = ws.uz;
     const double r0x = ws.r0x, r0y = ws.r0y, r0z = ws.r0z;
+    const double k = sv.k;
+    const float kt = (float)sv.kt;
+    float* vxp = reinterpret_cast<float*>(st.vx);
+    float* vyp = reinterpret_cast<float*>(st.vy);
+    float* vzp = reinterpret_cast<float*>(st.vz);
+    float* q2p = reinterpret_cast<float*>(st.q2);
+    float* nqp = reinterpret_cast<float*>(st.nq);
+    float* qxp = reinterpret_cast<float*>(st.qx);
+    float* qyp = reinterpret_cast<float*>(st.qy);
+    float* qzp = reinterpret_cast<float*>(st.qz);
 #pragma unroll
-    for (int i = 0; i < P; ++i) {
-        int id = sv.tile_perm[(long long)t * kPrTile + lane + 32 * i];
-        double x = id >= 0 ? sv.px[id] : p0x;
-        double y = id >= 0 ? sv.py[id] : p0y;
-        double z = id >= 0 ? sv.pz[id] : p0z;
-        double qx = x - r0x, qy = y - r0y, qz = z - r0z;
+    for (int i = 0; i < kPrPpl; ++i) {
+        const long long s = (long long)t * kPrTile + lane + 32 * i;
+        double qx = sv.tpx[s] - r0x, qy = sv.tpy[s] - r0y, qz = sv.tpz[s] - r0z;
         double qn = sqrt(qx * qx + qy * qy + qz * qz);
         double vx = qx - qn * ux, vy = qy - qn * uy, vz = qz - qn * uz;
-        ls.vx[i] = (float)(-2.0 * sv.k * vx);
-        ls.vy[i] = (float)(-2.0 * sv.k * vy);
-        ls.vz[i] = (float)(-2.0 * sv.k * vz);
-        ls.q2[i] = (float)(2.0 * qn);
+        vxp[i] = (float)(-2.0 * k * vx);
+        vyp[i] = (float)(-2.0 * k * vy);
+        vzp[i] = (float)(-2.0 * k * vz);
+        q2p[i] = FAST ? (float)(0.5 / qn) : (float)(2.0 * qn);
         if (UNIFORM) {
-            ls.nq[i] = (float)(2.0 * ((double)sv.unx * qx + (double)sv.uny * qy + (double)sv.unz * qz));
+            nqp[i] = (float)(2.0 * ((double)sv.unx * qx + (double)sv.uny * qy + (double)sv.unz * qz));
         } else {
-            // The prepared record carries 2n, so 2 n.q = (2n).q.
-            ls.qx[i] = (float)qx;
-            ls.qy[i] = (float)qy;
-            ls.qz[i] = (float)qz;
+            qxp[i] = (float)qx;
+            qyp[i] = (float)qy;
+            qzp[i] = (float)qz;
         }
+        // Base phase k|q| reduced to turns in FP64; sin/cos of the fraction.
+        double turns = sv.kt * qn;
+        float fr = (float)(turns - rint(turns));
+        float sp, cp;
+        sincospif(2.0f * fr, &sp, &cp);
+        ws.ph[i][lane] = make_float2(-kt * sp, kt * cp);
     }
 }
 
-// Multiplies the lane's two-float sums by (k/2pi) i exp(i k |q|) in FP64 and
-// adds them to the item's slots, then clears the sums.
-template <int P>
+// Multiplies the lane's two-float sums by the chunk phasor in FP64 and adds
+// them to the item's slots (tile-slot order), then clears the sums.
 __device__ __forceinline__ void flush_points(const PrSolve& sv, int t, int g, int lane,
-                                             WarpShared<P>& ws) {
-    const size_t m = (size_t)sv.n_pix;
-    double* base = sv.partial + (size_t)g * 4 * m;
-    const double r0x = ws.r0x, r0y = ws.r0y, r0z = ws.r0z;
-#pragma unroll 1
-    for (int i = 0; i < P; ++i) {
-        int id = sv.tile_perm[(long long)t * kPrTile + lane + 32 * i];
-        if (id >= 0) {
-            double qx = sv.px[id] - r0x, qy = sv.py[id] - r0y, qz = sv.pz[id] - r0z;
-            double qn = sqrt(qx * qx + qy * qy + qz * qz);
-            double turns = sv.kt * qn;
-            double f = turns - rint(turns);
-            double sp, cp;
-            sincospi(2.0 * f, &sp, &cp);
-            double phr = -sv.kt * sp, phi = sv.kt * cp;
-            double v[4];
+                                             WarpShared& ws) {
+    const size_t slots = (size_t)sv.n_tiles * kPrTile;
+    double* base = sv.partial + (size_t)g * 4 * slots;
+#pragma unroll 2
+    for (int i = 0; i < kPrPpl; ++i) {
+        const size_t s = (size_t)t * kPrTile + lane + 32 * i;
+        const float2 ph = ws.ph[i][lane];
+        const double phr = ph.x, phi = ph.y;
+        double v[4];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) v[c] = (double)ws.hi[i * 4 + c][lane] + (double)ws.lo[i * 4 + c][lane];
-            base[0 * m + id] += v[0] * phr - v[1] * phi;
-            base[1 * m + id] += v[0] * phi + v[1] * phr;
-            base[2 * m + id] += v[2] * phr - v[3] * phi;
-            base[3 * m + id] += v[2] * phi + v[3] * phr;
+        for (int c = 0; c < 4; ++c) {
+            v[c] = (double)ws.hi[i * 4 + c][lane] + (double)ws.lo[i * 4 + c][lane];
+            ws.hi[i * 4 + c][lane] = 0.f;
+            ws.lo[i * 4 + c][lane] = 0.f;
         }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) ws.hi[i * 4 + c][lane] = ws.lo[i * 4 + c][lane] = 0.f;
+        base[0 * slots + s] += v[0] * phr - v[1] * phi;
+        base[1 * slots + s] += v[0] * phi + v[1] * phr;
+        base[2 * slots + s] += v[2] * phr - v[3] * phi;
+        base[3 * slots + s] += v[2] * phi + v[3] * phr;
     }
 }
 
 // Prepares the stage's rays for the item direction (lane j handles rays
 // j, j+32).
-template <int P>
 __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, const PrSolve& sv,
-                                           const WarpShared<P>& ws) {
+                                           const WarpShared& ws) {
     const double ux = ws.ux, uy = ws.uy, uz = ws.uz;
     for (int j = lane; j < len; j += 32) {
         const PrRawRay r = buf[j];
@@ -459,13 +513,13 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
         double tx = r.rx - ur * ux, ty = r.ry - ur * uy, tz = r.rz - ur * uz;
         double perp2 = tx * tx + ty * ty + tz * tz;
         double turns = -sv.kt * ur;
-        double f = turns - rint(turns);
+        float f = (float)(turns - rint(turns));
         float sn, cs;
-        sincospif(2.0f * (float)f, &sn, &cs);
+        sincospif(2.0f * f, &sn, &cs);
         float rxf = (float)r.rx, ryf = (float)r.ry, rzf = (float)r.rz;
+        float w = (float)(-2.0 * ur);
         float4 a = make_float4(rxf, ryf, rzf, (float)(sv.k * perp2));
-        float4 b = make_float4((float)(-2.0 * ur), -2.f * (r.nx * rxf + r.ny * ryf + r.nz * rzf),
-                               r.nl, 0.f);
+        float4 b = make_float4(w, -2.f * (r.nx * rxf + r.ny * ryf + r.nz * rzf), r.nl, -w);
         float4 e = make_float4(r.es_re * cs - r.es_im * sn, r.es_re * sn + r.es_im * cs,
                                r.ep_re * cs - r.ep_im * sn, r.ep_re * sn + r.ep_im * cs);
         float4 nn = make_float4(2.f * r.nx, 2.f * r.ny, 2.f * r.nz, 0.f);
@@ -477,14 +531,13 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
     }
 }
 
-// The pair sweep: every lane runs the stage's rays against its P points,
-// then folds its FP32 partials into the two-float accumulators.
-template <int P, bool UNIFORM>
+// SFU sweep: one point per FP32 instruction, rcp.approx for the reciprocal.
+template <bool UNIFORM>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
-                                            LaneState<P, UNIFORM>& ls, WarpShared<P>& ws) {
+                                            ScalarState<UNIFORM>& ls, WarpShared& ws) {
     const float4* rec = reinterpret_cast<const float4*>(buf);
 #pragma unroll
-    for (int i = 0; i < P; ++i)
+    for (int i = 0; i < kPrPpl; ++i)
 #pragma unroll
         for (int c = 0; c < 4; ++c) ls.acc[i][c] = 0.f;
 #pragma unroll 1
@@ -495,7 +548,7 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
         float4 nn = make_float4(0.f, 0.f, 0.f, 0.f);
         if (!UNIFORM) nn = rec[4 * j + 3];
 #pragma unroll
-        for (int i = 0; i < P; ++i) {
+        for (int i = 0; i < kPrPpl; ++i) {
             float num = fmaf(ls.vx[i], a.x, a.w);
             num = fmaf(ls.vy[i], a.y, num);
             num = fmaf(ls.vz[i], a.z, num);
@@ -519,13 +572,79 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
         }
     }
 #pragma unroll
-    for (int i = 0; i < P; ++i)
+    for (int i = 0; i < kPrPpl; ++i)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             float hi = ws.hi[i * 4 + c][lane], lo = ws.lo[i * 4 + c][lane];
             two_sum_acc(hi, lo, ls.acc[i][c]);
             ws.hi[i * 4 + c][lane] = hi;
             ws.lo[i * 4 + c][lane] = lo;
+        }
+}
+
+// Packed sweep: two points per f32x2 instruction, series reciprocal.
+template <bool UNIFORM>
+__device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
+                                            PackedState<UNIFORM>& ls, WarpShared& ws) {
+    constexpr int H = kPrPpl / 2;
+    const float4* rec = reinterpret_cast<const float4*>(buf);
+#pragma unroll
+    for (int i = 0; i < H; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ls.acc[i][c] = f2(0.f);
+#pragma unroll 1
+    for (int j = 0; j < len; ++j) {
+        const float4 a = rec[4 * j + 0];
+        const float4 b = rec[4 * j + 1];
+        const float4 e = rec[4 * j + 2];
+        float4 nn = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!UNIFORM) nn = rec[4 * j + 3];
+        const float2 ax = f2(a.x), ay = f2(a.y), az = f2(a.z), aw = f2(a.w);
+        const float2 wn = f2(b.w), gg = f2(b.y), nl = f2(b.z);
+        const float2 ex = f2(e.x), ey = f2(e.y), ez = f2(e.z), ew = f2(e.w);
+        const float2 ney = f2(-e.y), new_ = f2(-e.w);
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            float2 num = __ffma2_rn(ls.vx[i], ax, aw);
+            num = __ffma2_rn(ls.vy[i], ay, num);
+            num = __ffma2_rn(ls.vz[i], az, num);
+            // 1/(2|q| - 2u.rho) = r0 / (1 - e), e = 2u.rho r0 ~ r0 (1 + e + e^2)
+            const float2 ep = __fmul2_rn(wn, ls.q2[i]);
+            const float2 rd = __ffma2_rn(ls.q2[i], __ffma2_rn(ep, ep, ep), ls.q2[i]);
+            const float2 th = __fmul2_rn(num, rd);
+            float s0, c0, s1, c1;
+            __sincosf(th.x, &s0, &c0);
+            __sincosf(th.y, &s1, &c1);
+            float2 gq;
+            if (UNIFORM) {
+                gq = __fadd2_rn(ls.nq[i], gg);
+            } else {
+                gq = __ffma2_rn(f2(nn.x), ls.qx[i],
+                                __ffma2_rn(f2(nn.y), ls.qy[i], __ffma2_rn(f2(nn.z), ls.qz[i], gg)));
+            }
+            const float2 obl = __ffma2_rn(gq, rd, nl);
+            const float2 amp = __fmul2_rn(obl, rd);
+            const float2 ac = __fmul2_rn(amp, f2(c0, c1));
+            const float2 as = __fmul2_rn(amp, f2(s0, s1));
+            ls.acc[i][0] = __ffma2_rn(ex, ac, __ffma2_rn(ney, as, ls.acc[i][0]));
+            ls.acc[i][1] = __ffma2_rn(ex, as, __ffma2_rn(ey, ac, ls.acc[i][1]));
+            ls.acc[i][2] = __ffma2_rn(ez, ac, __ffma2_rn(new_, as, ls.acc[i][2]));
+            ls.acc[i][3] = __ffma2_rn(ez, as, __ffma2_rn(ew, ac, ls.acc[i][3]));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < H; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float2 v = ls.acc[i][c];
+            float hi0 = ws.hi[(2 * i) * 4 + c][lane], lo0 = ws.lo[(2 * i) * 4 + c][lane];
+            float hi1 = ws.hi[(2 * i + 1) * 4 + c][lane], lo1 = ws.lo[(2 * i + 1) * 4 + c][lane];
+            two_sum_acc(hi0, lo0, v.x);
+            two_sum_acc(hi1, lo1, v.y);
+            ws.hi[(2 * i) * 4 + c][lane] = hi0;
+            ws.lo[(2 * i) * 4 + c][lane] = lo0;
+            ws.hi[(2 * i + 1) * 4 + c][lane] = hi1;
+            ws.lo[(2 * i + 1) * 4 + c][lane] = lo1;
         }
 }
 
@@ -555,8 +674,8 @@ __device__ __forceinline__ int chunk_of(const int* __restrict__ begin, int n_chu
 }
 
 // Processes one (tile, ray-range) item; false if a bounded wait ran out.
-template <int P, bool UNIFORM>
-__device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, WarpShared<P>& ws,
+template <bool UNIFORM, bool FAST>
+__device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, WarpShared& ws,
                              int lane) {
     const int t = (int)(local % sv.n_tiles);
     const int g = (int)(local / sv.n_tiles);
@@ -568,9 +687,10 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
     const int* __restrict__ cb = sv.chunk_begin;
 
 #pragma unroll
-    for (int i = 0; i < P * 4; ++i) ws.hi[i][lane] = ws.lo[i][lane] = 0.f;
+    for (int i = 0; i < kPrPpl * 4; ++i) ws.hi[i][lane] = ws.lo[i][lane] = 0.f;
 
-    LaneState<P, UNIFORM> ls;
+    using State = typename std::conditional<FAST, PackedState<UNIFORM>, ScalarState<UNIFORM>>::type;
+    State st;
     int cur_chunk = -1;
     int pos = r0;
     int c = chunk_of(cb, n_chunks, pos);
@@ -598,7 +718,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
             return false;
         }
         if (c != cur_chunk) {
-            if (cur_chunk >= 0) flush_points<P>(sv, t, g, lane, ws);
+            if (cur_chunk >= 0) flush_points(sv, t, g, lane, ws);
             __syncwarp();
             if (lane == 0) {
                 const double p0x = sv.tile_center[3 * t], p0y = sv.tile_center[3 * t + 1],
@@ -615,12 +735,12 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
                 ws.r0z = r0z;
             }
             __syncwarp();
-            setup_points<P, UNIFORM>(sv, t, lane, ws, ls);
+            setup_points<UNIFORM, FAST>(sv, t, lane, ws, st);
             cur_chunk = c;
         }
-        prep_stage<P>(wp.buf[b], len, lane, sv, ws);
+        prep_stage(wp.buf[b], len, lane, sv, ws);
         __syncwarp();
-        sweep_stage<P, UNIFORM>(wp.buf[b], len, lane, ls, ws);
+        sweep_stage<UNIFORM>(wp.buf[b], len, lane, st, ws);
         // Order this stage's generic-proxy accesses before the next bulk
         // copy into the same buffer.
         fence_proxy_async();
@@ -631,21 +751,22 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
         len = nlen;
         b ^= 1;
     }
-    flush_points<P>(sv, t, g, lane, ws);
+    flush_points(sv, t, g, lane, ws);
     __syncwarp();
     return true;
 }
 
-// Every solve in `solves` must have uniform_normal == UNIFORM.
-template <int P, bool UNIFORM>
+// Every solve in `solves` must match the kernel's variant (normal mode and
+// sweep); solves[s].item_begin is the prefix sum of the item counts.
+template <bool UNIFORM, bool FAST>
 __global__ void __launch_bounds__(kPrWarpsPerCta * 32, 3)
 pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long n_items,
                      unsigned long long* __restrict__ counter, int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     PrRawRay* bufs = reinterpret_cast<PrRawRay*>(smem) + warp * 2 * kPrStage;
-    WarpShared<P>* wsh = reinterpret_cast<WarpShared<P>*>(
-                             smem + kPrWarpsPerCta * 2 * kPrStage * sizeof(PrRawRay)) + warp;
+    WarpShared* wsh = reinterpret_cast<WarpShared*>(
+                          smem + kPrWarpsPerCta * 2 * kPrStage * sizeof(PrRawRay)) + warp;
     WarpPipe wp;
     wp.buf[0] = bufs;
     wp.buf[1] = bufs + kPrStage;
@@ -664,11 +785,15 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
         if (lane == 0) item = (long long)atomicAdd(counter, 1ull);
         item = __shfl_sync(kFull, item, 0);
         if (item >= n_items) break;
-        int s = 0;
-        while (s + 1 < n_solves && solves[s + 1].item_begin <= item) ++s;
-        const PrSolve& sv = solves[s];
+        int lo = 0, hi = n_solves - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (solves[mid].item_begin <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const PrSolve& sv = solves[lo];
         const long long local = item - sv.item_begin;
-        const bool ok = process_item<P, UNIFORM>(sv, local, wp, *wsh, lane);
+        const bool ok = process_item<UNIFORM, FAST>(sv, local, wp, *wsh, lane);
         if (!ok) {
             if (lane == 0) atomicExch(err, 1);
             break;
@@ -677,7 +802,14 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
 }
 
 constexpr size_t kPrSmemBytes = (size_t)kPrWarpsPerCta * 2 * kPrStage * sizeof(PrRawRay) +
-                                (size_t)kPrWarpsPerCta * sizeof(WarpShared<kPrPpl>);
+                                (size_t)kPrWarpsPerCta * sizeof(WarpShared);
+
+using PrKernel = void (*)(const PrSolve*, int, long long, unsigned long long*, int*);
+
+PrKernel pr_kernel(bool uniform, bool fast) {
+    if (uniform) return fast ? pr_persistent_kernel<true, true> : pr_persistent_kernel<true, false>;
+    return fast ? pr_persistent_kernel<false, true> : pr_persistent_kernel<false, false>;
+}
 
 // ---------------------------------------------------------------------------
 // Host side
@@ -737,6 +869,80 @@ double phase_bound(double k, double a, double b, double d) {
     return k * (b * b + 2.0 * a * b) / (2.0 * den);
 }
 
+// Per-solve planning scratch carved from the arena.
+struct SolveBufs {
+    double* sum;
+    uint64_t *pk_in, *pk_out;
+    int *pi_in, *pi_out;
+    int* tile_perm;
+    double *tpx, *tpy, *tpz, *tile_center;
+    unsigned long long* amax;
+    uint64_t *rk_in, *rk_out;
+    int *ri_in, *ri_out, *flags, *run;
+    int* chunk_begin;
+    double* chunk_center;
+    int* n_chunks;
+    PrRawRay* recs;
+    double* partial;
+};
+
+void carve(Arena& a, SolveBufs& b, int n, int m, int n_tiles, int groups, int sum_blocks) {
+    const size_t slots = (size_t)n_tiles * kPrTile;
+    b.sum = a.take<double>((size_t)sum_blocks * kSumFields);
+    b.pk_in = a.take<uint64_t>(m);
+    b.pk_out = a.take<uint64_t>(m);
+    b.pi_in = a.take<int>(m);
+    b.pi_out = a.take<int>(m);
+    b.tile_perm = a.take<int>(slots);
+    b.tpx = a.take<double>(slots);
+    b.tpy = a.take<double>(slots);
+    b.tpz = a.take<double>(slots);
+    b.tile_center = a.take<double>(3 * (size_t)n_tiles);
+    b.amax = a.take<unsigned long long>(1);
+    b.rk_in = a.take<uint64_t>(n);
+    b.rk_out = a.take<uint64_t>(n);
+    b.ri_in = a.take<int>(n);
+    b.ri_out = a.take<int>(n);
+    b.flags = a.take<int>(n);
+    b.run = a.take<int>(n);
+    b.chunk_begin = a.take<int>((size_t)n + 1);
+    b.chunk_center = a.take<double>(3 * (size_t)n);
+    b.n_chunks = a.take<int>(1);
+    b.recs = a.take<PrRawRay>(n);
+    b.partial = a.take<double>((size_t)groups * 4 * slots);
+}
+
+struct HostSolveInfo {
+    double f[kSumFields];
+    double k = 0, d_lo = 0, rc[3], pc[3], rlo[3], rhi[3], plo[3], phi[3];
+    Frame fr{};
+};
+
+// Pinned host area layout: [per-solve summaries][per-solve amax][per-solve
+// n_chunks][error word][solve tables].
+struct HostLayout {
+    size_t sum_off, amax_off, nch_off, err_off, tab_off, total;
+};
+
+HostLayout host_layout(int count, int sum_blocks) {
+    HostLayout L;
+    size_t off = 0;
+    L.sum_off = off;
+    off = align_up(off + (size_t)count * sum_blocks * kSumFields * sizeof(double), 256);
+    L.amax_off = off;
+    off = align_up(off + (size_t)count * sizeof(double), 256);
+    L.nch_off = off;
+    off = align_up(off + (size_t)count * sizeof(int), 256);
+    L.err_off = off;
+    off = align_up(off + 64, 256);
+    L.tab_off = off;
+    off = align_up(off + (size_t)count * sizeof(PrSolve), 256);
+    L.total = off;
+    return L;
+}
+
+int sum_blocks_for(int num_sms) { return std::min(512, std::max(1, 2 * num_sms)); }
+
 }  // namespace
 
 const char* const kRouteReasons[kRouteReasonCount] = {
@@ -753,6 +959,7 @@ Status PrWorkspace::ensure_host(size_t bytes) {
     if (host) cudaFreeHost(host);
     host = nullptr;
     host_bytes = 0;
+    host_err = nullptr;
     XK_CUDA_TRY(cudaMallocHost(&host, bytes));
     host_bytes = bytes;
     return Status::Ok();
@@ -769,321 +976,397 @@ void PrWorkspace::release() {
     if (host) cudaFreeHost(host);
     host = nullptr;
     host_bytes = 0;
+    host_err = nullptr;
 }
 
-Status pr_solve_enqueue(const RaysDev& rays, size_t n_rays_, const PixDev& pix, size_t n_pix_,
-                        const FieldDev& out, PrWorkspace& ws, cudaStream_t stream, int num_sms,
-                        PrReport* rep, const PrOptions& opt) {
-    PrReport local;
-    PrReport& R = rep ? *rep : local;
-    R = PrReport();
-    if (n_pix_ == 0) return Status::Ok();
-    if (n_rays_ == 0) {
-        R.routed_f64 = true;
-        R.route_reason = 1;  // no rays
-        return Status::Ok();
-    }
-    if (n_rays_ > (size_t)INT32_MAX / 2 || n_pix_ > (size_t)INT32_MAX / 2)
-        return Status::Err(XK_ERR_INVALID, "too many rays or screen points for one solve");
-    const int n = (int)n_rays_, m = (int)n_pix_;
-    const int n_tiles = (m + kPrTile - 1) / kPrTile;
-
-    // Groups: enough items to keep every warp of the persistent grid busy,
-    // at least 4 stages of rays per item, partial slots within 4 GiB.
-    int groups = opt.groups;
-    if (groups <= 0) {
-        long long want_items = (long long)num_sms * 12 * 16;
-        groups = (int)std::max<long long>(1, (want_items + n_tiles - 1) / n_tiles);
-        groups = std::min(groups, std::max(1, n / (4 * kPrStage)));
-        long long cap = (4LL << 30) / (32LL * m);
-        groups = (int)std::max<long long>(1, std::min<long long>(groups, cap));
-        groups = std::min(groups, 256);
-    }
-    R.groups = groups;
-
-    // --- arena -----------------------------------------------------------
-    const int sum_blocks = std::min(512, std::max(1, 2 * num_sms));
-    size_t cub_sort_n = 0, cub_sort_m = 0, cub_scan = 0;
-    XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, cub_sort_n, (uint64_t*)nullptr,
-                                                (uint64_t*)nullptr, (int*)nullptr, (int*)nullptr, n));
-    XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, cub_sort_m, (uint64_t*)nullptr,
-                                                (uint64_t*)nullptr, (int*)nullptr, (int*)nullptr, m));
-    XK_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, cub_scan, (int*)nullptr, (int*)nullptr, n));
-    XK_TRY(ws.cub_tmp.ensure(std::max(cub_sort_n, std::max(cub_sort_m, cub_scan)) + 256));
-
+Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t stream, int num_sms,
+               const PrOptions& opt, std::vector<PrPlan>& plans, int* kernels) {
+    plans.assign(count, PrPlan());
+    int nk = 0;
+    const int sum_blocks = sum_blocks_for(num_sms);
+    std::vector<int> n_tiles(count, 0), groups(count, 0);
+    size_t cub_need = 0;
     size_t need = 0;
-    {
-        Arena a{nullptr};
-        a.take<double>((size_t)sum_blocks * kSumFields);
-        a.take<uint64_t>(m); a.take<uint64_t>(m); a.take<int>(m); a.take<int>(m);
-        a.take<int>((size_t)n_tiles * kPrTile); a.take<double>(3 * (size_t)n_tiles);
-        a.take<unsigned long long>(1);
-        a.take<uint64_t>(n); a.take<uint64_t>(n); a.take<int>(n); a.take<int>(n);
-        a.take<int>(n); a.take<int>(n);
-        a.take<int>((size_t)n + 1); a.take<double>(3 * (size_t)n); a.take<int>(1);
-        a.take<PrRawRay>(n);
-        a.take<double>((size_t)groups * 4 * m);
-        need = a.off + 256;
+    for (int s = 0; s < count; ++s) {
+        PrPlan& P = plans[s];
+        P.out = in[s].out;
+        P.m = (int)in[s].m;
+        if (in[s].n == 0 || in[s].m == 0) {
+            P.routed = true;
+            P.route_reason = 1;
+            continue;
+        }
+        if (in[s].n > (size_t)INT32_MAX / 2 || in[s].m > (size_t)INT32_MAX / 2)
+            return Status::Err(XK_ERR_INVALID, "too many rays or screen points for one solve");
+        const int n = (int)in[s].n, m = (int)in[s].m;
+        n_tiles[s] = (m + kPrTile - 1) / kPrTile;
+        int g = opt.groups;
+        if (g <= 0) {
+            // Enough items to keep every resident warp busy, at least four
+            // stages of rays per item, partial slots within 1 GiB.
+            long long want = (long long)num_sms * 12 * opt.items_per_warp;
+            g = (int)std::max<long long>(1, (want + n_tiles[s] - 1) / n_tiles[s]);
+            g = std::min(g, std::max(1, n / (4 * kPrStage)));
+            long long cap = (1LL << 30) / (32LL * n_tiles[s] * kPrTile);
+            g = (int)std::max<long long>(1, std::min<long long>(g, cap));
+            g = std::min(g, 4096);
+        }
+        groups[s] = g;
+        size_t c1 = 0, c2 = 0, c3 = 0;
+        XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, c1, (uint64_t*)nullptr,
+                                                    (uint64_t*)nullptr, (int*)nullptr,
+                                                    (int*)nullptr, n));
+        XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, c2, (uint64_t*)nullptr,
+                                                    (uint64_t*)nullptr, (int*)nullptr,
+                                                    (int*)nullptr, m));
+        XK_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, c3, (int*)nullptr, (int*)nullptr, n));
+        cub_need = std::max(cub_need, std::max(c1, std::max(c2, c3)));
+        Arena a{nullptr, need};
+        SolveBufs b;
+        carve(a, b, n, m, n_tiles[s], g, sum_blocks);
+        need = a.off;
     }
-    XK_TRY(ws.arena.ensure(need));
-    Arena a{ws.arena.as<char>()};
-    double* d_sum = a.take<double>((size_t)sum_blocks * kSumFields);
-    uint64_t* d_pk_in = a.take<uint64_t>(m);
-    uint64_t* d_pk_out = a.take<uint64_t>(m);
-    int* d_pi_in = a.take<int>(m);
-    int* d_pi_out = a.take<int>(m);
-    int* d_tile_perm = a.take<int>((size_t)n_tiles * kPrTile);
-    double* d_tile_center = a.take<double>(3 * (size_t)n_tiles);
-    unsigned long long* d_amax = a.take<unsigned long long>(1);
-    uint64_t* d_rk_in = a.take<uint64_t>(n);
-    uint64_t* d_rk_out = a.take<uint64_t>(n);
-    int* d_ri_in = a.take<int>(n);
-    int* d_ri_out = a.take<int>(n);
-    int* d_flags = a.take<int>(n);
-    int* d_run = a.take<int>(n);
-    int* d_chunk_begin = a.take<int>((size_t)n + 1);
-    double* d_chunk_center = a.take<double>(3 * (size_t)n);
-    int* d_nchunks = a.take<int>(1);
-    PrRawRay* d_recs = a.take<PrRawRay>(n);
-    double* d_partial = a.take<double>((size_t)groups * 4 * m);
+    XK_TRY(ws.cub_tmp.ensure(cub_need + 256));
+    XK_TRY(ws.arena.ensure(need + 256));
+    const HostLayout HL = host_layout(count, sum_blocks);
+    XK_TRY(ws.ensure_host(HL.total));
+    char* hbase = static_cast<char*>(ws.host);
+    double* h_sum = reinterpret_cast<double*>(hbase + HL.sum_off);
+    double* h_amax = reinterpret_cast<double*>(hbase + HL.amax_off);
+    int* h_nch = reinterpret_cast<int*>(hbase + HL.nch_off);
 
-    // Pinned readback area: block summaries | solve descriptor | status words.
-    const size_t host_sum_bytes = align_up((size_t)sum_blocks * kSumFields * sizeof(double), 256);
-    XK_TRY(ws.ensure_host(host_sum_bytes + align_up(sizeof(PrSolve), 256) + 256));
-    double* h_sum = static_cast<double*>(ws.host);
-    PrSolve* h_sv = reinterpret_cast<PrSolve*>(static_cast<char*>(ws.host) + host_sum_bytes);
-    int* h_misc = reinterpret_cast<int*>(static_cast<char*>(ws.host) + host_sum_bytes +
-                                         align_up(sizeof(PrSolve), 256));
-
-    // --- 1. summary -------------------------------------------------------
-    summary_kernel<<<sum_blocks, 256, 0, stream>>>(rays, n, pix, m, d_sum);
-    XK_CUDA_TRY(cudaGetLastError());
-    XK_CUDA_TRY(cudaMemcpyAsync(h_sum, d_sum, (size_t)sum_blocks * kSumFields * sizeof(double),
-                                cudaMemcpyDeviceToHost, stream));
-    XK_CUDA_TRY(cudaStreamSynchronize(stream));
-    R.kernels += 1;
-    double f[kSumFields];
+    std::vector<SolveBufs> bufs(count);
     {
-        static const int ops[kSumFields] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 1, 2, 1, 1,
-                                            1, 2, 2, 2, 0, 0, 0, 1, 1, 1, 2, 2, 2};
-        for (int i = 0; i < kSumFields; ++i) {
-            double v = h_sum[i];
-            for (int bk = 1; bk < sum_blocks; ++bk) {
-                double w = h_sum[bk * kSumFields + i];
-                v = ops[i] == 0 ? v + w : (ops[i] == 1 ? std::min(v, w) : std::max(v, w));
-            }
-            f[i] = v;
+        size_t off = 0;
+        for (int s = 0; s < count; ++s) {
+            if (plans[s].routed) continue;
+            Arena a{ws.arena.as<char>(), off};
+            carve(a, bufs[s], (int)in[s].n, (int)in[s].m, n_tiles[s], groups[s], sum_blocks);
+            off = a.off;
         }
     }
-    if (!(f[9] == f[10])) {
-        R.routed_f64 = true;
-        R.route_reason = 2;  // rays of different energies
-        return Status::Ok();
-    }
-    const double energy = f[9];
-    const double k = (energy / kChbar) * 1e7;
-    if (!(k > 0) || !std::isfinite(k)) {
-        R.routed_f64 = true;
-        R.route_reason = 3;  // non-positive energy
-        return Status::Ok();
-    }
-    const bool uniform_normal = f[11] == f[14] && f[12] == f[15] && f[13] == f[16];
-    const double rlo[3] = {f[3], f[4], f[5]}, rhi[3] = {f[6], f[7], f[8]};
-    const double plo[3] = {f[20], f[21], f[22]}, phi[3] = {f[23], f[24], f[25]};
-    const double d_lo = box_distance(rlo, rhi, plo, phi);
-    if (!(d_lo > 0)) {
-        R.routed_f64 = true;
-        R.route_reason = 4;  // ray and screen bounding boxes overlap
-        return Status::Ok();
-    }
-    const double rc[3] = {f[0] / n, f[1] / n, f[2] / n};
-    const double pc[3] = {f[17] / m, f[18] / m, f[19] / m};
 
-    // Frame: u0 from the ray centroid towards the screen centroid.
-    Frame fr{};
-    double u0[3] = {pc[0] - rc[0], pc[1] - rc[1], pc[2] - rc[2]};
-    if (u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2] == 0) u0[2] = 1;
-    normalize3(u0);
-    double helper[3] = {std::fabs(u0[0]) < 0.9 ? 1.0 : 0.0, std::fabs(u0[0]) < 0.9 ? 0.0 : 1.0, 0.0};
-    double dot = helper[0] * u0[0] + helper[1] * u0[1] + helper[2] * u0[2];
-    double e1[3] = {helper[0] - dot * u0[0], helper[1] - dot * u0[1], helper[2] - dot * u0[2]};
-    normalize3(e1);
-    double e2[3] = {u0[1] * e1[2] - u0[2] * e1[1], u0[2] * e1[0] - u0[0] * e1[2],
-                    u0[0] * e1[1] - u0[1] * e1[0]};
-    for (int i = 0; i < 3; ++i) {
-        fr.e1[i] = e1[i];
-        fr.e2[i] = e2[i];
-        fr.u0[i] = u0[i];
+    // --- A. summaries ------------------------------------------------------
+    bool any = false;
+    for (int s = 0; s < count; ++s) {
+        if (plans[s].routed) continue;
+        any = true;
+        summary_kernel<<<sum_blocks, 256, 0, stream>>>(in[s].rays, (int)in[s].n, in[s].pix,
+                                                        (int)in[s].m, bufs[s].sum);
+        XK_CUDA_TRY(cudaGetLastError());
+        XK_CUDA_TRY(cudaMemcpyAsync(h_sum + (size_t)s * sum_blocks * kSumFields, bufs[s].sum,
+                                    (size_t)sum_blocks * kSumFields * sizeof(double),
+                                    cudaMemcpyDeviceToHost, stream));
+        ++nk;
+    }
+    if (!any) {
+        if (kernels) *kernels += nk;
+        return Status::Ok();
+    }
+    XK_CUDA_TRY(cudaStreamSynchronize(stream));
+
+    std::vector<HostSolveInfo> info(count);
+    for (int s = 0; s < count; ++s) {
+        PrPlan& P = plans[s];
+        if (P.routed) continue;
+        HostSolveInfo& I = info[s];
+        const double* hs = h_sum + (size_t)s * sum_blocks * kSumFields;
+        for (int i = 0; i < kSumFields; ++i) {
+            double v = hs[i];
+            for (int bk = 1; bk < sum_blocks; ++bk) {
+                double w = hs[bk * kSumFields + i];
+                v = h_sum_ops[i] == 0 ? v + w : (h_sum_ops[i] == 1 ? std::min(v, w) : std::max(v, w));
+            }
+            I.f[i] = v;
+        }
+        const double* f = I.f;
+        if (!(f[9] == f[10])) {
+            P.routed = true;
+            P.route_reason = 2;
+            continue;
+        }
+        I.k = (f[9] / kChbar) * 1e7;
+        if (!(I.k > 0) || !std::isfinite(I.k)) {
+            P.routed = true;
+            P.route_reason = 3;
+            continue;
+        }
+        P.uniform_normal = f[11] == f[14] && f[12] == f[15] && f[13] == f[16];
+        for (int a = 0; a < 3; ++a) {
+            I.rlo[a] = f[3 + a];
+            I.rhi[a] = f[6 + a];
+            I.plo[a] = f[20 + a];
+            I.phi[a] = f[23 + a];
+            I.rc[a] = f[a] / (double)in[s].n;
+            I.pc[a] = f[17 + a] / (double)in[s].m;
+        }
+        I.d_lo = box_distance(I.rlo, I.rhi, I.plo, I.phi);
+        if (!(I.d_lo > 0)) {
+            P.routed = true;
+            P.route_reason = 4;
+            continue;
+        }
+        double u0[3] = {I.pc[0] - I.rc[0], I.pc[1] - I.rc[1], I.pc[2] - I.rc[2]};
+        if (u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2] == 0) u0[2] = 1;
+        normalize3(u0);
+        double helper[3] = {std::fabs(u0[0]) < 0.9 ? 1.0 : 0.0, std::fabs(u0[0]) < 0.9 ? 0.0 : 1.0,
+                            0.0};
+        double dot = helper[0] * u0[0] + helper[1] * u0[1] + helper[2] * u0[2];
+        double e1[3] = {helper[0] - dot * u0[0], helper[1] - dot * u0[1], helper[2] - dot * u0[2]};
+        normalize3(e1);
+        double e2[3] = {u0[1] * e1[2] - u0[2] * e1[1], u0[2] * e1[0] - u0[0] * e1[2],
+                        u0[0] * e1[1] - u0[1] * e1[0]};
+        for (int i = 0; i < 3; ++i) {
+            I.fr.e1[i] = e1[i];
+            I.fr.e2[i] = e2[i];
+            I.fr.u0[i] = u0[i];
+        }
     }
 
-    // --- 2. screen tiles ----------------------------------------------------
-    {
-        Frame pf = fr;
-        pf.ox = pc[0]; pf.oy = pc[1]; pf.oz = pc[2];
-        const double* axes[3] = {e1, e2, u0};
+    // --- B. screen tiles ----------------------------------------------------
+    any = false;
+    for (int s = 0; s < count; ++s) {
+        PrPlan& P = plans[s];
+        if (P.routed) continue;
+        any = true;
+        HostSolveInfo& I = info[s];
+        SolveBufs& B = bufs[s];
+        const int m = (int)in[s].m;
+        Frame pf = I.fr;
+        pf.ox = I.pc[0];
+        pf.oy = I.pc[1];
+        pf.oz = I.pc[2];
+        const double* axes[3] = {I.fr.e1, I.fr.e2, I.fr.u0};
+        const double qmax[3] = {65535.0, 65535.0, 2097151.0};
         for (int ax = 0; ax < 3; ++ax) {
             double mn, mx;
-            project_box(plo, phi, pc, axes[ax], &mn, &mx);
+            project_box(I.plo, I.phi, I.pc, axes[ax], &mn, &mx);
             pf.lo[ax] = mn;
-            pf.scale[ax] = (mx > mn) ? 2097151.0 / (mx - mn) : 0.0;
+            pf.scale[ax] = (mx > mn) ? qmax[ax] / (mx - mn) : 0.0;
         }
-        pixel_keys_kernel<<<(m + 255) / 256, 256, 0, stream>>>(pix, m, pf, d_pk_in, d_pi_in);
+        pixel_keys_kernel<<<(m + 255) / 256, 256, 0, stream>>>(in[s].pix, m, pf, B.pk_in, B.pi_in);
         XK_CUDA_TRY(cudaGetLastError());
         size_t tmp = ws.cub_tmp.bytes;
-        XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp.ptr, tmp, d_pk_in, d_pk_out, d_pi_in,
-                                                    d_pi_out, m, 0, 63, stream));
-        XK_CUDA_TRY(cudaMemsetAsync(d_amax, 0, sizeof(unsigned long long), stream));
-        int warps_blocks = (n_tiles * 32 + 255) / 256;
-        tile_kernel<<<warps_blocks, 256, 0, stream>>>(pix, m, n_tiles, d_pi_out, d_tile_perm,
-                                                       d_tile_center, d_amax);
+        XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp.ptr, tmp, B.pk_in, B.pk_out, B.pi_in,
+                                                    B.pi_out, m, 0, 53, stream));
+        XK_CUDA_TRY(cudaMemsetAsync(B.amax, 0, sizeof(unsigned long long), stream));
+        tile_kernel<<<(n_tiles[s] * 32 + 255) / 256, 256, 0, stream>>>(
+            in[s].pix, m, n_tiles[s], B.pi_out, B.tile_perm, B.tpx, B.tpy, B.tpz, B.tile_center,
+            B.amax);
         XK_CUDA_TRY(cudaGetLastError());
-        XK_CUDA_TRY(cudaMemcpyAsync(h_sum, d_amax, sizeof(double), cudaMemcpyDeviceToHost, stream));
-        XK_CUDA_TRY(cudaStreamSynchronize(stream));
-        R.kernels += 2;
+        XK_CUDA_TRY(cudaMemcpyAsync(h_amax + s, B.amax, sizeof(double), cudaMemcpyDeviceToHost,
+                                    stream));
+        nk += 2;
     }
-    const double a_max = h_sum[0] * 1.001;
+    if (any) XK_CUDA_TRY(cudaStreamSynchronize(stream));
 
-    // --- 3. ray cells -----------------------------------------------------
-    CellGrid cg{};
-    cg.fr = fr;
-    cg.fr.ox = rc[0]; cg.fr.oy = rc[1]; cg.fr.oz = rc[2];
-    double ext[3];
-    {
-        const double* axes[3] = {e1, e2, u0};
+    // --- C. ray chunks ------------------------------------------------------
+    for (int s = 0; s < count; ++s) {
+        PrPlan& P = plans[s];
+        if (P.routed) continue;
+        HostSolveInfo& I = info[s];
+        SolveBufs& B = bufs[s];
+        const int n = (int)in[s].n;
+        const double a_max = h_amax[s] * 1.001;
+        const double k = I.k;
+        CellGrid cg{};
+        cg.fr = I.fr;
+        cg.fr.ox = I.rc[0];
+        cg.fr.oy = I.rc[1];
+        cg.fr.oz = I.rc[2];
+        double ext[3];
+        const double* axes[3] = {I.fr.e1, I.fr.e2, I.fr.u0};
         for (int ax = 0; ax < 3; ++ax) {
             double mn, mx;
-            project_box(rlo, rhi, rc, axes[ax], &mn, &mx);
+            project_box(I.rlo, I.rhi, I.rc, axes[ax], &mn, &mx);
             cg.fr.lo[ax] = mn;
             ext[ax] = mx - mn;
         }
-    }
-    auto cell_radius = [&](double h, double cell[3]) {
-        double s = 0;
+        auto cell_radius = [&](double h, double cell[3]) {
+            double sq = 0;
+            for (int ax = 0; ax < 3; ++ax) {
+                cell[ax] = ext[ax] <= h ? ext[ax] : h;
+                sq += 0.25 * cell[ax] * cell[ax];
+            }
+            return std::sqrt(sq);
+        };
+        double cell[3];
+        double h_hi = 2.0 * std::max(ext[0], std::max(ext[1], ext[2])) + 1e-300;
+        double h_lo = 0.0;
+        if (phase_bound(k, a_max, cell_radius(h_hi, cell), I.d_lo) <= opt.phase_budget) {
+            h_lo = h_hi;
+        } else {
+            for (int it = 0; it < 200; ++it) {
+                double h = 0.5 * (h_lo + h_hi);
+                if (phase_bound(k, a_max, cell_radius(h, cell), I.d_lo) <= opt.phase_budget) h_lo = h;
+                else h_hi = h;
+            }
+        }
+        const double h = h_lo;
+        const double b_max = cell_radius(h, cell);
+        if (!(h > 0)) {
+            P.routed = true;
+            P.route_reason = 5;
+            continue;
+        }
+        bool too_fine = false;
         for (int ax = 0; ax < 3; ++ax) {
-            cell[ax] = ext[ax] <= h ? ext[ax] : h;
-            s += 0.25 * cell[ax] * cell[ax];
+            cg.cell[ax] = cell[ax];
+            double cnt = cell[ax] > 0 ? std::floor(ext[ax] / cell[ax]) + 1.0 : 1.0;
+            if (cnt > 2097151.0) too_fine = true;
+            cg.n[ax] = (long long)cnt;
         }
-        return std::sqrt(s);
-    };
-    double cell[3];
-    double h_hi = 2.0 * std::max(ext[0], std::max(ext[1], ext[2])) + 1e-300;
-    double h_lo = 0.0;
-    if (phase_bound(k, a_max, cell_radius(h_hi, cell), d_lo) <= opt.phase_budget) {
-        h_lo = h_hi;
-    } else {
-        for (int it = 0; it < 200; ++it) {
-            double h = 0.5 * (h_lo + h_hi);
-            if (phase_bound(k, a_max, cell_radius(h, cell), d_lo) <= opt.phase_budget) h_lo = h;
-            else h_hi = h;
+        if (too_fine) {
+            P.routed = true;
+            P.route_reason = 6;
+            continue;
         }
-    }
-    const double h = h_lo;
-    const double b_max = cell_radius(h, cell);
-    if (!(h > 0)) {
-        R.routed_f64 = true;
-        R.route_reason = 5;  // no cell size meets the phase budget
-        return Status::Ok();
-    }
-    for (int ax = 0; ax < 3; ++ax) {
-        cg.cell[ax] = cell[ax];
-        double cnt = cell[ax] > 0 ? std::floor(ext[ax] / cell[ax]) + 1.0 : 1.0;
-        if (cnt > 2097151.0) {
-            R.routed_f64 = true;
-            R.route_reason = 6;  // ray cell grid too fine
-            return Status::Ok();
-        }
-        cg.n[ax] = (long long)cnt;
-    }
-    R.phase_bound = phase_bound(k, a_max, b_max, d_lo);
+        P.phase_bound = phase_bound(k, a_max, b_max, I.d_lo);
+        // |e| = |u.rho| / |q| <= b / (d_lo - b): the series reciprocal's
+        // argument.
+        P.rcp_bound = b_max / std::max(I.d_lo - b_max, 1e-300);
+        P.fast = opt.sweep == 1 || (opt.sweep < 0 && P.rcp_bound <= kSeriesRcpBound);
 
-    ray_keys_kernel<<<(n + 255) / 256, 256, 0, stream>>>(rays, n, cg, d_rk_in, d_ri_in);
-    XK_CUDA_TRY(cudaGetLastError());
-    {
+        ray_keys_kernel<<<(n + 255) / 256, 256, 0, stream>>>(in[s].rays, n, cg, B.rk_in, B.ri_in);
+        XK_CUDA_TRY(cudaGetLastError());
         size_t tmp = ws.cub_tmp.bytes;
-        XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp.ptr, tmp, d_rk_in, d_rk_out, d_ri_in,
-                                                    d_ri_out, n, 0, 63, stream));
-    }
-    head_flags_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_rk_out, n, d_flags);
-    XK_CUDA_TRY(cudaGetLastError());
-    {
-        size_t tmp = ws.cub_tmp.bytes;
-        XK_CUDA_TRY(cub::DeviceScan::InclusiveSum(ws.cub_tmp.ptr, tmp, d_flags, d_run, n, stream));
-    }
-    chunk_table_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_rk_out, d_flags, d_run, n, cg,
-                                                             d_chunk_begin, d_chunk_center, d_nchunks);
-    XK_CUDA_TRY(cudaGetLastError());
-    records_kernel<<<(n + 255) / 256, 256, 0, stream>>>(rays, n, d_ri_out, d_run, d_chunk_center,
-                                                         d_recs);
-    XK_CUDA_TRY(cudaGetLastError());
-    R.kernels += 5;
+        XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp.ptr, tmp, B.rk_in, B.rk_out, B.ri_in,
+                                                    B.ri_out, n, 0, 63, stream));
+        head_flags_kernel<<<(n + 255) / 256, 256, 0, stream>>>(B.rk_out, n, B.flags);
+        XK_CUDA_TRY(cudaGetLastError());
+        tmp = ws.cub_tmp.bytes;
+        XK_CUDA_TRY(cub::DeviceScan::InclusiveSum(ws.cub_tmp.ptr, tmp, B.flags, B.run, n, stream));
+        chunk_table_kernel<<<(n + 255) / 256, 256, 0, stream>>>(B.rk_out, B.flags, B.run, n, cg,
+                                                                 B.chunk_begin, B.chunk_center,
+                                                                 B.n_chunks);
+        XK_CUDA_TRY(cudaGetLastError());
+        records_kernel<<<(n + 255) / 256, 256, 0, stream>>>(in[s].rays, n, B.ri_out, B.run,
+                                                             B.chunk_center, B.recs);
+        XK_CUDA_TRY(cudaGetLastError());
+        nk += 5;
 
-    // --- 4. persistent sweep ------------------------------------------------
-    PrSolve sv{};
-    sv.recs = d_recs;
-    sv.chunk_begin = d_chunk_begin;
-    sv.chunk_center = d_chunk_center;
-    sv.n_chunks_dev = d_nchunks;
-    sv.tile_perm = d_tile_perm;
-    sv.tile_center = d_tile_center;
-    sv.px = pix.x;
-    sv.py = pix.y;
-    sv.pz = pix.z;
-    sv.partial = d_partial;
-    sv.item_begin = 0;
-    sv.n_items = (long long)n_tiles * groups;
-    sv.n_rays = n;
-    sv.n_pix = m;
-    sv.n_tiles = n_tiles;
-    sv.groups = groups;
-    sv.k = k;
-    sv.kt = k / (2.0 * kPi);
-    sv.uniform_normal = uniform_normal ? 1 : 0;
-    {
-        // The common normal, read back from the summary (min == max).
-        sv.unx = (float)f[11];
-        sv.uny = (float)f[12];
-        sv.unz = (float)f[13];
+        PrSolve& D = P.dev;
+        D.recs = B.recs;
+        D.chunk_begin = B.chunk_begin;
+        D.chunk_center = B.chunk_center;
+        D.n_chunks_dev = B.n_chunks;
+        D.tpx = B.tpx;
+        D.tpy = B.tpy;
+        D.tpz = B.tpz;
+        D.tile_center = B.tile_center;
+        D.partial = B.partial;
+        D.item_begin = 0;
+        D.n_items = (long long)n_tiles[s] * groups[s];
+        D.n_rays = n;
+        D.n_tiles = n_tiles[s];
+        D.groups = groups[s];
+        D.k = k;
+        D.kt = k / (2.0 * kPi);
+        D.unx = (float)I.f[11];
+        D.uny = (float)I.f[12];
+        D.unz = (float)I.f[13];
+        P.tile_perm = B.tile_perm;
+        P.n_tiles = n_tiles[s];
+        P.groups = groups[s];
+        P.n_chunks_host = h_nch + s;
+        *P.n_chunks_host = 0;
     }
-    XK_TRY(ws.solves.ensure(sizeof(PrSolve)));
-    XK_TRY(ws.ctrl.ensure(64));
-    *h_sv = sv;
-    XK_CUDA_TRY(cudaMemcpyAsync(ws.solves.ptr, h_sv, sizeof(PrSolve), cudaMemcpyHostToDevice, stream));
-    XK_CUDA_TRY(cudaMemsetAsync(ws.ctrl.ptr, 0, 64, stream));
-    XK_CUDA_TRY(cudaMemsetAsync(d_partial, 0, (size_t)groups * 4 * m * sizeof(double), stream));
+    if (kernels) *kernels += nk;
+    return Status::Ok();
+}
 
-    auto kern = uniform_normal ? pr_persistent_kernel<kPrPpl, true>
-                               : pr_persistent_kernel<kPrPpl, false>;
-    XK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kPrSmemBytes));
-    int per_sm = 0;
-    XK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPrWarpsPerCta * 32,
-                                                              kPrSmemBytes));
-    per_sm = std::max(per_sm, 1);
-    long long grid = (long long)num_sms * per_sm;
-    long long max_ctas = (sv.n_items + kPrWarpsPerCta - 1) / kPrWarpsPerCta;
-    grid = std::max<long long>(1, std::min(grid, max_ctas));
-    unsigned long long* d_counter = reinterpret_cast<unsigned long long*>(ws.ctrl.ptr);
-    int* d_err = reinterpret_cast<int*>(static_cast<char*>(ws.ctrl.ptr) + 8);
+Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStream_t stream,
+                          int num_sms, bool time_kernels, PrExecReport* rep) {
+    PrExecReport local;
+    PrExecReport& R = rep ? *rep : local;
+    const int count = (int)plans.size();
+    const HostLayout HL = host_layout(count, sum_blocks_for(num_sms));
+    XK_TRY(ws.ensure_host(HL.total));
+    char* hbase = static_cast<char*>(ws.host);
+    PrSolve* h_tab = reinterpret_cast<PrSolve*>(hbase + HL.tab_off);
+    int* h_nch = reinterpret_cast<int*>(hbase + HL.nch_off);
+    ws.host_err = reinterpret_cast<int*>(hbase + HL.err_off);
+    *ws.host_err = 0;
+    XK_TRY(ws.solves.ensure(std::max<size_t>(1, count) * sizeof(PrSolve)));
+    XK_TRY(ws.ctrl.ensure(256));
     if (!ws.ev[0]) XK_CUDA_TRY(cudaEventCreate(&ws.ev[0]));
     if (!ws.ev[1]) XK_CUDA_TRY(cudaEventCreate(&ws.ev[1]));
-    XK_CUDA_TRY(cudaEventRecord(ws.ev[0], stream));
-    kern<<<(unsigned)grid, kPrWarpsPerCta * 32, kPrSmemBytes, stream>>>(
-        reinterpret_cast<const PrSolve*>(ws.solves.ptr), 1, sv.n_items, d_counter, d_err);
-    XK_CUDA_TRY(cudaGetLastError());
-    XK_CUDA_TRY(cudaEventRecord(ws.ev[1], stream));
-    finalize_kernel<<<(m + 255) / 256, 256, 0, stream>>>(d_partial, groups, m, out);
-    XK_CUDA_TRY(cudaGetLastError());
-    R.kernels += 2;
+    unsigned long long* d_counters = reinterpret_cast<unsigned long long*>(ws.ctrl.ptr);
+    int* d_err = reinterpret_cast<int*>(static_cast<char*>(ws.ctrl.ptr) + 128);
+    XK_CUDA_TRY(cudaMemsetAsync(ws.ctrl.ptr, 0, 256, stream));
 
-    XK_CUDA_TRY(cudaMemcpyAsync(h_misc, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    XK_CUDA_TRY(cudaMemcpyAsync(h_misc + 1, d_nchunks, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    XK_CUDA_TRY(cudaStreamSynchronize(stream));
-    if (h_misc[0] != 0)
-        return Status::Err(XK_ERR_TIMEOUT, "persistent kernel: bounded wait for a ray stage ran out");
-    XK_CUDA_TRY(cudaEventElapsedTime(&R.main_kernel_ms, ws.ev[0], ws.ev[1]));
-    R.n_tiles = n_tiles;
-    R.n_chunks = h_misc[1];
-    R.n_items = sv.n_items;
+    // Group the planned solves by kernel variant into contiguous tables.
+    struct Launch {
+        int first, count;
+        long long items;
+        bool uniform, fast;
+    };
+    std::vector<Launch> launches;
+    int tab = 0;
+    for (int variant = 0; variant < 4; ++variant) {
+        const bool uniform = (variant & 1) != 0, fast = (variant & 2) != 0;
+        Launch L{tab, 0, 0, uniform, fast};
+        for (int s = 0; s < count; ++s) {
+            PrPlan& P = plans[s];
+            if (P.routed || P.uniform_normal != uniform || P.fast != fast) continue;
+            P.dev.item_begin = L.items;
+            h_tab[tab++] = P.dev;
+            L.items += P.dev.n_items;
+            L.count++;
+            const size_t slots = (size_t)P.n_tiles * kPrTile;
+            XK_CUDA_TRY(cudaMemsetAsync(P.dev.partial, 0,
+                                        (size_t)P.groups * 4 * slots * sizeof(double), stream));
+        }
+        if (L.count) launches.push_back(L);
+    }
+    if (tab == 0) return Status::Ok();
+    XK_CUDA_TRY(cudaMemcpyAsync(ws.solves.ptr, h_tab, (size_t)tab * sizeof(PrSolve),
+                                cudaMemcpyHostToDevice, stream));
+    if (time_kernels) XK_CUDA_TRY(cudaEventRecord(ws.ev[0], stream));
+    int li = 0;
+    for (const Launch& L : launches) {
+        PrKernel kern = pr_kernel(L.uniform, L.fast);
+        XK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kPrSmemBytes));
+        int per_sm = 0;
+        XK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPrWarpsPerCta * 32,
+                                                                  kPrSmemBytes));
+        per_sm = std::max(per_sm, 1);
+        long long grid = (long long)num_sms * per_sm;
+        grid = std::max<long long>(1, std::min(grid, (L.items + kPrWarpsPerCta - 1) / kPrWarpsPerCta));
+        kern<<<(unsigned)grid, kPrWarpsPerCta * 32, kPrSmemBytes, stream>>>(
+            reinterpret_cast<const PrSolve*>(ws.solves.ptr) + L.first, L.count, L.items,
+            d_counters + li, d_err);
+        XK_CUDA_TRY(cudaGetLastError());
+        R.kernels += 1;
+        R.n_items += L.items;
+        ++li;
+    }
+    if (time_kernels) XK_CUDA_TRY(cudaEventRecord(ws.ev[1], stream));
+    for (int s = 0; s < count; ++s) {
+        PrPlan& P = plans[s];
+        if (P.routed) continue;
+        const int slots = P.n_tiles * kPrTile;
+        finalize_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(P.dev.partial, P.tile_perm,
+                                                                 P.groups, slots, P.out);
+        XK_CUDA_TRY(cudaGetLastError());
+        XK_CUDA_TRY(cudaMemcpyAsync(h_nch + s, P.dev.n_chunks_dev, sizeof(int),
+                                    cudaMemcpyDeviceToHost, stream));
+        R.kernels += 1;
+    }
+    XK_CUDA_TRY(cudaMemcpyAsync(ws.host_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    return Status::Ok();
+}
+
+Status pr_execute_finish(std::vector<PrPlan>& plans, PrWorkspace& ws, PrExecReport* rep) {
+    if (rep && rep->kernels > 0 && ws.ev[0]) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ws.ev[0], ws.ev[1]) == cudaSuccess) rep->main_kernel_ms = ms;
+    }
+    for (auto& P : plans)
+        if (!P.routed && P.n_chunks_host) P.n_chunks = *P.n_chunks_host;
+    if (ws.host_err && *ws.host_err != 0)
+        return Status::Err(XK_ERR_TIMEOUT, "persistent kernel: a bounded wait for a ray stage ran out");
     return Status::Ok();
 }
 

@@ -1,6 +1,8 @@
 // FP32 phase-reduced Kirchhoff path: planner + persistent kernel.
 #pragma once
 
+#include <vector>
+
 #include "xk_internal.cuh"
 
 namespace xk {
@@ -14,20 +16,9 @@ constexpr int kPrTile = 32 * kPrPpl;  // screen points per tile (one warp)
 // Planner knobs.
 struct PrOptions {
     double phase_budget = 256.0;  // bound on |FP32 residual phase| [rad]
-    double min_rays_per_chunk = 2.0;
-    int groups = 0;  // ray groups per tile; 0 = automatic
-};
-
-struct PrReport {
-    int kernels = 0;
-    bool routed_f64 = false;
-    int route_reason = 0;  // index into kRouteReasons
-    int n_tiles = 0;
-    int n_chunks = 0;
-    long long n_items = 0;
-    double phase_bound = 0.0;
-    int groups = 0;
-    float main_kernel_ms = 0.f;
+    int groups = 0;               // ray groups per tile; 0 = automatic
+    int sweep = -1;               // -1 automatic, 0 SFU reciprocal, 1 packed + Newton
+    long long items_per_warp = 16;  // target items per resident warp (automatic groups)
 };
 
 // Reasons a solve is routed to the FP64 path (xk_route_reason).
@@ -45,39 +36,79 @@ struct __align__(16) PrRawRay {
 };
 static_assert(sizeof(PrRawRay) == 64, "record is 64 bytes");
 
-// Device-side description of one planned solve.
+// Device-side description of one planned solve (read by the persistent
+// kernel).
 struct PrSolve {
     const PrRawRay* recs;         // [n_rays] in chunk order
     const int* chunk_begin;       // [n_chunks + 1]
     const double* chunk_center;   // [3 * n_chunks]
     const int* n_chunks_dev;      // scalar
-    const int* tile_perm;         // [n_tiles * kPrTile], -1 = padding slot
+    const double *tpx, *tpy, *tpz;  // screen points in tile-slot order (padding = tile centre)
     const double* tile_center;    // [3 * n_tiles]
-    const double *px, *py, *pz;   // screen points (original order)
-    double* partial;              // [groups][4][n_pix]
-    long long item_begin;         // first global item of this solve
+    double* partial;              // [groups][4][n_tiles * kPrTile], tile-slot order
+    long long item_begin;         // first global item of this solve in its launch
     long long n_items;            // n_tiles * groups
-    int n_rays, n_pix, n_tiles, groups;
+    int n_rays, n_tiles, groups;
     double k;                     // wavenumber [1/mm]
-    double kt;                    // k / (2 pi)  (turns per mm)
-    int uniform_normal;
-    float unx, uny, unz;          // the common normal when uniform_normal
+    double kt;                    // k / (2 pi)
+    float unx, uny, unz;          // the common normal (uniform-normal kernels)
+};
+
+// One solve's inputs (device pointers).
+struct PrSolveIn {
+    RaysDev rays;
+    size_t n;
+    PixDev pix;
+    size_t m;
+    FieldDev out;
+};
+
+// Host-side result of planning one solve.
+struct PrPlan {
+    bool routed = false;
+    int route_reason = 0;
+    bool uniform_normal = false;
+    bool fast = false;  // packed sweep with Newton reciprocal
+    int n_tiles = 0, groups = 0, n_chunks = 0;
+    double phase_bound = 0.0, rcp_bound = 0.0;
+    PrSolve dev{};
+    const int* tile_perm = nullptr;  // slot -> original screen point, -1 = padding
+    int m = 0;
+    FieldDev out{};
+    int* n_chunks_host = nullptr;    // filled after execution
+};
+
+struct PrExecReport {
+    int kernels = 0;
+    float main_kernel_ms = 0.f;
+    long long n_items = 0;
 };
 
 struct PrWorkspace {
     DevBuf arena;
     DevBuf cub_tmp;
-    DevBuf solves;  // PrSolve array for the persistent launch
-    DevBuf ctrl;    // counter + error flag
-    cudaEvent_t ev[2] = {nullptr, nullptr};  // bracket the pair kernel
-    void* host = nullptr;  // pinned readback area
+    DevBuf solves;  // PrSolve tables for the persistent launches
+    DevBuf ctrl;    // item counters + error flag
+    cudaEvent_t ev[2] = {nullptr, nullptr};  // bracket the pair kernels
+    void* host = nullptr;  // pinned readback / upload area
     size_t host_bytes = 0;
+    int* host_err = nullptr;  // error word copied back by the last execution
     Status ensure_host(size_t bytes);
     void release();
 };
 
-Status pr_solve_enqueue(const RaysDev& rays, size_t n_rays, const PixDev& pix, size_t n_pix,
-                        const FieldDev& out, PrWorkspace& ws, cudaStream_t stream, int num_sms,
-                        PrReport* rep, const PrOptions& opt = PrOptions());
+// Plans `count` solves in one pass (three host synchronisations for the
+// whole batch). Plans reference memory in ws.arena until the next call.
+Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t stream, int num_sms,
+               const PrOptions& opt, std::vector<PrPlan>& plans, int* kernels);
+
+// Enqueues the sweep of every non-routed plan: per kernel variant one
+// persistent launch over all of its solves, then one finalize per solve.
+// Does not synchronise; safe to capture in a CUDA graph.
+Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStream_t stream,
+                          int num_sms, bool time_kernels, PrExecReport* rep);
+
+// After the stream is synchronised: error flag and chunk counts.
+Status pr_execute_finish(std::vector<PrPlan>& plans, PrWorkspace& ws, PrExecReport* rep);
 
 }  // namespace xk

@@ -79,6 +79,10 @@ class GpuContext:
         _lib.check(rc)
         return cls(h, False)
 
+    def set_option(self, name: str, value: float):
+        """Tuning knob of the F32PR path (phase_budget, sweep, groups, items_per_warp)."""
+        _lib.check(_lib.load().xk_set_option(self._h, name.encode(), float(value)), self._h)
+
     def adapter_name(self) -> str:
         return _lib.load().xk_device_name(self._h).decode()
 

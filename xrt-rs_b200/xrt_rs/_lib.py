@@ -67,6 +67,7 @@ class XkStats(ctypes.Structure):
         ("main_kernel_ms", ctypes.c_double),
         ("groups", ctypes.c_int),
         ("routed_reason", ctypes.c_int),
+        ("sweep", ctypes.c_int),
     ]
 
     def to_dict(self):
@@ -83,6 +84,7 @@ _SIGNATURES = {
     "xk_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "xk_version": (ctypes.c_char_p, []),
     "xk_route_reason": (ctypes.c_char_p, [ctypes.c_int]),
+    "xk_set_option": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double]),
     "xk_diffraction_integral": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels),
         ctypes.c_size_t, ctypes.POINTER(XkField), ctypes.c_int, ctypes.POINTER(XkStats)]),
