@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--sweep", type=int, default=-1, help="-1 auto, 0 SFU reciprocal, 1 packed")
+    ap.add_argument("--phase-budget", type=float, default=256.0)
     return ap.parse_args()
 
 
@@ -216,6 +218,8 @@ def main():
     ctx = xrt_rs.GpuContext.new(dev.index)
     if ctx is None:
         raise RuntimeError("no CUDA device")
+    ctx.set_option("sweep", args.sweep)
+    ctx.set_option("phase_budget", args.phase_budget)
 
     rays, screen = synth.config1(seed=rank, n_rays=args.rays, grid=args.grid)
     fields = xrt_rs.RAY_FIELDS
