@@ -179,6 +179,35 @@ int xk_kirchhoff_gpu(xk_ctx* ctx, const xk_gpu_ray* rays, size_t n_rays,
 int xk_kirchhoff_auto(const xk_gpu_ray* rays, size_t n_rays, const xk_gpu_pixel* pixels,
                       size_t n_pix, double* out);
 
+/* ---- allocation-free FP64 solve ---------------------------------------------
+ *
+ * No counterpart in the reference. For callers that cannot let a library
+ * allocate device memory: programs whose device memory is all owned by their
+ * own pool allocator, and loops that cannot pay for cudaMalloc's implicit
+ * synchronisation on every call. It computes exactly what XK_PATH_F64
+ * computes (same kernels), with its scratch in a fixed array inside the
+ * library instead of context buffers, and it calls no cudaMalloc, cudaFree
+ * or other allocating routine.
+ *
+ * - rays, pixels and out hold DEVICE pointers on the current device; the
+ *   work is enqueued on `stream` (cudaStream_t, NULL = default stream) and
+ *   the results are ready once that stream is synchronised.
+ * - n_rays may not exceed XK_NOALLOC_MAX_RAYS: larger requests return
+ *   XK_ERR_BUDGET and launch nothing. n_pix is not limited.
+ * - The fixed scratch is XK_NOALLOC_SCRATCH_BYTES (32 MiB) of device memory,
+ *   held by every GPU on which the library's FP64 code is loaded until exit.
+ * - The first call on a device looks up the scratch's device address with
+ *   that device current; make that first call before any stream capture.
+ * - All calls share the one scratch array and it keeps the last call's
+ *   contents (every byte a call reads is written earlier in the same call, so
+ *   nothing needs clearing). Calls that overlap on the GPU — from several
+ *   host threads, or on several streams without ordering between them — race
+ *   on the scratch and corrupt each other's results: serialise them. */
+#define XK_NOALLOC_MAX_RAYS 131072
+#define XK_NOALLOC_SCRATCH_BYTES (32u << 20)
+int xk_diffraction_f64_noalloc(const xk_rays* rays, size_t n_rays, const xk_pixels* pixels,
+                               size_t n_pix, xk_field* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -226,3 +226,118 @@ Status f64_enqueue(const RaysDev& rays, size_t n_rays, const PixDev& pix, size_t
 }
 
 }  // namespace xk
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the FP64 path.
+//
+// Some callers cannot let a library call cudaMalloc: applications that have
+// handed all device memory to their own pool allocator, and loops that cannot
+// afford cudaMalloc's implicit device-wide synchronisation and latency on
+// every call. For them xk_diffraction_f64_noalloc runs the same FP64 kernels
+// as XK_PATH_F64, but its scratch (the packed ray records and the split-ray
+// partial sums) lives in the fixed array below instead of context buffers.
+// The array is a module global: every GPU on which this library's FP64 code
+// is loaded holds its kNoAllocScratchBytes until the process exits.
+// ---------------------------------------------------------------------------
+
+namespace xk {
+namespace {
+
+constexpr size_t kNoAllocMaxRays = XK_NOALLOC_MAX_RAYS;
+constexpr size_t kNoAllocRayBytes = kNoAllocMaxRays * sizeof(RayRec64);  // 16 MiB
+constexpr size_t kNoAllocPartialDoubles = (size_t)2 << 20;                // 16 MiB
+constexpr size_t kNoAllocScratchBytes = kNoAllocRayBytes + kNoAllocPartialDoubles * sizeof(double);
+static_assert(kNoAllocScratchBytes == XK_NOALLOC_SCRATCH_BYTES, "header and scratch size agree");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once with that
+// device current (a host-side reference to the symbol is not a device address).
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+}  // namespace
+}  // namespace xk
+
+extern "C" int xk_diffraction_f64_noalloc(const xk_rays* rays, size_t n_rays,
+                                          const xk_pixels* pixels, size_t n_pix, xk_field* out,
+                                          void* stream) {
+    using namespace xk;
+    if (n_pix == 0) return XK_OK;
+    if (!pixels || !pixels->x || !pixels->y || !pixels->z || !out || !out->es_re ||
+        !out->es_im || !out->ep_re || !out->ep_im)
+        return XK_ERR_INVALID;
+    if (n_rays > 0 && (!rays || !rays->x || !rays->y || !rays->z || !rays->nx || !rays->ny ||
+                       !rays->nz || !rays->nl || !rays->es_re || !rays->es_im || !rays->ep_re ||
+                       !rays->ep_im || !rays->energy))
+        return XK_ERR_INVALID;
+    if (n_rays > kNoAllocMaxRays) return XK_ERR_BUDGET;
+
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        cudaGetLastError();
+        return XK_ERR_NO_DEVICE;
+    }
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return XK_ERR_CUDA;
+            }
+            g_noalloc_addr[dev] = p;
+        }
+        base = g_noalloc_addr[dev];
+    }
+    int num_sms = 0;
+    if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return XK_ERR_CUDA;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    FieldDev fd{out->es_re, out->es_im, out->ep_re, out->ep_im};
+    PixDev pd{pixels->x, pixels->y, pixels->z};
+    if (n_rays == 0) {
+        zero_field_kernel<<<(unsigned)((n_pix + 255) / 256), 256, 0, s>>>(fd, n_pix);
+        return cudaGetLastError() == cudaSuccess ? XK_OK : XK_ERR_CUDA;
+    }
+    RaysDev rd{rays->x, rays->y, rays->z, rays->nx, rays->ny, rays->nz, rays->nl,
+               rays->es_re, rays->es_im, rays->ep_re, rays->ep_im, rays->energy};
+    RayRec64* packed = static_cast<RayRec64*>(base);
+    double* partial_area =
+        reinterpret_cast<double*>(static_cast<unsigned char*>(base) + kNoAllocRayBytes);
+
+    // Same split rule as the allocating path, capped so the partials fit the
+    // fixed area; every partial is written before it is read, so the area
+    // never needs clearing.
+    const size_t pix_per_cta = (size_t)kF64Threads * kF64Ppt;
+    const size_t pix_ctas = (n_pix + pix_per_cta - 1) / pix_per_cta;
+    const size_t want = (size_t)num_sms * 32;
+    size_t splits = (want + pix_ctas - 1) / pix_ctas;
+    size_t max_splits = (n_rays + kF64Stage - 1) / kF64Stage;
+    if (splits > max_splits) splits = max_splits;
+    const size_t fit = kNoAllocPartialDoubles / (4 * n_pix);
+    if (splits > fit) splits = fit;
+    if (splits > 65535) splits = 65535;
+    if (splits < 1) splits = 1;
+    size_t rays_per_split = (n_rays + splits - 1) / splits;
+    rays_per_split = (rays_per_split + kF64Stage - 1) / kF64Stage * kF64Stage;
+    splits = (n_rays + rays_per_split - 1) / rays_per_split;
+    double* partials = splits > 1 ? partial_area : nullptr;
+
+    f64_pack_kernel<<<(unsigned)((n_rays + 255) / 256), 256, 0, s>>>(rd, n_rays, packed);
+    if (cudaGetLastError() != cudaSuccess) return XK_ERR_CUDA;
+    dim3 grid((unsigned)pix_ctas, (unsigned)splits);
+    f64_pairs_kernel<<<grid, kF64Threads, 0, s>>>(packed, n_rays, rays_per_split, pd, n_pix, fd,
+                                                   partials);
+    if (cudaGetLastError() != cudaSuccess) return XK_ERR_CUDA;
+    if (splits > 1) {
+        f64_combine_kernel<<<(unsigned)((n_pix + 255) / 256), 256, 0, s>>>(partials, (int)splits,
+                                                                           n_pix, fd);
+        if (cudaGetLastError() != cudaSuccess) return XK_ERR_CUDA;
+    }
+    return XK_OK;
+}

@@ -95,6 +95,9 @@ _SIGNATURES = {
     "xk_kirchhoff_gpu": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.POINTER(XkGpuRay), ctypes.c_size_t, ctypes.POINTER(XkGpuPixel),
         ctypes.c_size_t, _dp]),
+    "xk_diffraction_f64_noalloc": (ctypes.c_int, [
+        ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels), ctypes.c_size_t,
+        ctypes.POINTER(XkField), ctypes.c_void_p]),
     "xk_kirchhoff_auto": (ctypes.c_int, [
         ctypes.POINTER(XkGpuRay), ctypes.c_size_t, ctypes.POINTER(XkGpuPixel), ctypes.c_size_t,
         _dp]),
