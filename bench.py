@@ -62,6 +62,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sweep", type=int, default=-1, help="-1 auto, 0 SFU reciprocal, 1 packed")
     ap.add_argument("--phase-budget", type=float, default=256.0)
+    ap.add_argument("--workload", choices=["single", "batch", "sweep"], default="single",
+                    help="single: the 2^20 x 512^2 solve (default); batch: 64 uneven solves; "
+                         "sweep: the energy x distance precision sweep")
+    ap.add_argument("--sweep-sample", type=int, default=64,
+                    help="screen points per cell checked against the CPU oracle")
+    ap.add_argument("--batch-count", type=int, default=64)
     return ap.parse_args()
 
 
@@ -196,10 +202,149 @@ def run_reference(args):
     return 0
 
 
+def run_batch(args):
+    """64 uneven solves: one persistent graph-captured launch vs a loop of
+    per-solve calls, both on device-resident inputs."""
+    import torch
+    import xrt_rs
+    from xrt_rs import synth
+
+    torch.cuda.set_device(0)
+    ctx = xrt_rs.GpuContext.new(0)
+    ctx.set_option("sweep", args.sweep)
+    ctx.set_option("phase_budget", args.phase_budget)
+    solves = synth.config3(seed=0, count=args.batch_count)
+    pairs = float(sum(len(r["x"]) * len(p["x"]) for r, p, _ in solves))
+    dev = []
+    for rays, screen, _ in solves:
+        d_r = [torch.from_numpy(rays[k]).cuda() for k in xrt_rs.RAY_FIELDS]
+        d_p = [torch.from_numpy(screen[k]).cuda() for k in "xyz"]
+        d_o = [torch.zeros(len(screen["x"]), dtype=torch.float64, device="cuda") for _ in range(4)]
+        dev.append((d_r, d_p, d_o))
+    stream = torch.cuda.current_stream()
+
+    def loop():
+        for d_r, d_p, d_o in dev:
+            xrt_rs.diffraction_integral_device(d_r, d_p, d_o, path="f32pr", ctx=ctx,
+                                               stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        loop()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        loop()
+    torch.cuda.synchronize()
+    loop_ms = 1e3 * (time.perf_counter() - t0) / args.steps
+
+    batch = xrt_rs.Batch([(d_r, d_p) for d_r, d_p, _ in dev], path="f32pr", ctx=ctx,
+                         device_outputs=[d_o for _, _, d_o in dev])
+    plan_ms = None
+    for _ in range(args.warmup):
+        batch.run()
+        plan_ms = batch.stats["plan_ms"]
+    exec_ms, wall_ms = [], []
+    for _ in range(args.steps):
+        batch.run()
+        exec_ms.append(batch.stats["exec_ms"])
+        wall_ms.append(batch.stats["wall_ms"])
+    ex = float(np.mean(exec_ms))
+    line = {
+        "workload": "batch", "metric": "Gpair/s over 64 uneven solves", "unit": UNIT,
+        "value": pairs / (ex / 1e3) / 1e9, "steps": args.steps, "warmup": args.warmup,
+        "pairs_per_step": pairs, "n_solves": len(solves),
+        "inputs": "device-resident for both arms",
+        "batch_graph_exec_ms": ex, "batch_run_wall_ms": float(np.mean(wall_ms)),
+        "batch_plan_ms": plan_ms, "loop_per_solve_calls_ms": loop_ms,
+        "loop_gpair_s": pairs / (loop_ms / 1e3) / 1e9,
+        "batch_plus_plan_gpair_s": pairs / ((ex + plan_ms) / 1e3) / 1e9,
+        "speedup_graph_exec_vs_loop": loop_ms / ex,
+        "routed_f64": batch.stats["routed_f64"], "kernels_per_run": batch.stats["kernels"],
+        "data": "synthetic: N log-uniform [1e3,1e6], M log-uniform [64,262144], E U(5,25) keV, "
+                "d U(500,10000) mm, sigma U(0.02,0.2) mm, R U(10,50) m",
+    }
+    print(json.dumps(line), flush=True)
+    batch.close()
+    ctx.close()
+    return 0
+
+
+def run_sweep(args):
+    """E in {1,5,10,20,30} keV x d in {100,1000,5000,20000} mm, 2^18 rays x 256^2.
+
+    Per cell: the FP32 phase-reduced field and the FP64 field on the GPU (full
+    screen, timed), and their errors on a seeded screen subsample against the
+    oracle evaluated with an extended-precision phase (CPU)."""
+    import torch
+    import xrt_rs
+    from oracle import oracle
+    from xrt_rs import synth
+
+    torch.cuda.set_device(0)
+    ctx = xrt_rs.GpuContext.new(0)
+    cells = []
+    for e in synth.CONFIG2_ENERGIES:
+        for d in synth.CONFIG2_DISTANCES:
+            rays, screen, meta = synth.config2_cell(e, d, seed=int(e) + int(d))
+            rl = [rays[k] for k in xrt_rs.RAY_FIELDS]
+            d_r = [torch.from_numpy(a).cuda() for a in rl]
+            d_p = [torch.from_numpy(screen[k]).cuda() for k in "xyz"]
+            m = len(screen["x"])
+            res = {}
+            for path in ("f32pr", "f64"):
+                d_o = [torch.zeros(m, dtype=torch.float64, device="cuda") for _ in range(4)]
+                xrt_rs.diffraction_integral_device(d_r, d_p, d_o, path=path, ctx=ctx)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                st = xrt_rs.diffraction_integral_device(d_r, d_p, d_o, path=path, ctx=ctx)
+                e1.record()
+                e1.synchronize()
+                res[path] = ([t.cpu().numpy() for t in d_o], e0.elapsed_time(e1), st)
+            sub, idx = synth.subsample_screen(screen, args.sweep_sample, seed=int(e + d))
+            exact = oracle.kahan_ld(rl, [sub["x"], sub["y"], sub["z"]])
+
+            def err(out):
+                a = np.concatenate([out[0][idx] + 1j * out[1][idx], out[2][idx] + 1j * out[3][idx]])
+                b = np.concatenate([exact[0] + 1j * exact[1], exact[2] + 1j * exact[3]])
+                ia = np.abs(a[: len(idx)]) ** 2 + np.abs(a[len(idx):]) ** 2
+                ib = np.abs(b[: len(idx)]) ** 2 + np.abs(b[len(idx):]) ** 2
+                return (float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                        float(np.linalg.norm(ia - ib) / np.linalg.norm(ib)))
+
+            pairs = float(len(rl[0])) * m
+            f32, f64 = res["f32pr"], res["f64"]
+            e32, e32i = err(f32[0])
+            e64, e64i = err(f64[0])
+            cells.append({
+                "energy_ev": e, "dist_mm": d, "sigma_mm": meta["sigma_mm"],
+                "radius_mm": meta["radius_mm"], "path": "f32pr" if f32[2]["path"] == 1 else "f64",
+                "n_chunks": f32[2]["n_chunks"], "sweep": f32[2]["sweep"],
+                "rel_l2_field": e32, "rel_l2_intensity": e32i,
+                "fp64_formula_rel_l2_field": e64, "fp64_formula_rel_l2_intensity": e64i,
+                "f32pr_gpair_s": pairs / f32[1] / 1e6, "fp64_gpair_s": pairs / f64[1] / 1e6,
+                "speedup": f64[1] / f32[1]})
+            print(json.dumps(cells[-1]), file=sys.stderr, flush=True)
+    worst = max(c["rel_l2_field"] for c in cells)
+    line = {"workload": "sweep", "metric": "rel L2 vs the extended-precision oracle per (E, d) cell",
+            "n_rays": 1 << 18, "screen": "256x256 grid +-1 mm", "sample_points": args.sweep_sample,
+            "worst_rel_l2_field": worst,
+            "worst_rel_l2_intensity": max(c["rel_l2_intensity"] for c in cells),
+            "min_speedup": min(c["speedup"] for c in cells), "cells": cells}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "sweep":
+        return run_sweep(args)
 
     import torch
     import xrt_rs

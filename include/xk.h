@@ -179,6 +179,127 @@ int xk_kirchhoff_gpu(xk_ctx* ctx, const xk_gpu_ray* rays, size_t n_rays,
 int xk_kirchhoff_auto(const xk_gpu_ray* rays, size_t n_rays, const xk_gpu_pixel* pixels,
                       size_t n_pix, double* out);
 
+/* ---- batches of solves ------------------------------------------------------
+ *
+ * Many independent solves of uneven sizes in one persistent launch. No
+ * counterpart in the reference, which solves one problem per call; each
+ * solve keeps the semantics of xk_diffraction_integral. */
+typedef struct xk_solve {
+    xk_rays rays;
+    size_t n_rays;
+    xk_pixels pixels;
+    size_t n_pix;
+    xk_field out;
+} xk_solve;
+
+enum {
+    XK_BATCH_DEVICE = 1,   /* every pointer in the solves is a device pointer */
+    XK_BATCH_NO_GRAPH = 2  /* enqueue the launches on each run instead of replaying a graph */
+};
+
+typedef struct xk_batch xk_batch;
+
+typedef struct xk_batch_stats {
+    double pairs;       /* sum of n_rays * n_pix */
+    double plan_ms;     /* host wall time of xk_batch_create (copies + planning) */
+    double exec_ms;     /* device time of the run's launches (CUDA events) */
+    double wall_ms;     /* host wall time of xk_batch_run incl. output copies */
+    int n_solves;
+    int routed_f64;     /* solves that ran on XK_PATH_F64 */
+    int kernels;        /* kernel launches per run */
+    int graph;          /* 1 if the run replayed a CUDA graph */
+    long long n_items;  /* FP32-PR work items per run */
+} xk_batch_stats;
+
+typedef struct xk_solve_plan {
+    int path, routed_reason, n_tiles, n_chunks, groups, sweep;
+    double phase_bound_rad;
+} xk_solve_plan;
+
+/* Copies host inputs to the device (unless XK_BATCH_DEVICE), plans every
+ * solve in one pass (three host synchronisations for the whole batch) and
+ * captures the execution — one persistent launch per kernel variant over all
+ * solves' items, then the per-solve reductions — in a CUDA graph. The solves'
+ * input and output buffers must stay valid until xk_batch_destroy. */
+int xk_batch_create(xk_ctx* ctx, const xk_solve* solves, size_t n, int path, int flags,
+                    xk_batch** out);
+
+/* Runs the batch (graph replay) and writes every solve's field to its `out`
+ * buffers; blocks until done. Repeated runs recompute the same inputs. */
+int xk_batch_run(xk_batch* batch, xk_batch_stats* stats);
+
+/* Plan of solve i (valid after xk_batch_create; chunk counts after a run). */
+int xk_batch_solve_plan(const xk_batch* batch, size_t i, xk_solve_plan* out);
+
+void xk_batch_destroy(xk_batch* batch);
+
+/* ---- serving: continuous batching --------------------------------------------
+ *
+ * No counterpart in the reference (one blocking call per solve). A server
+ * accepts solves from any thread; a worker admits them while the admitted
+ * set fits an HBM budget, plans them, and runs them in epochs: each epoch is
+ * one persistent launch over work items of every admitted request (a fair
+ * share each), so a request that arrives while others run joins the next
+ * epoch. A request's result does not depend on what else is in flight. */
+typedef struct xk_server xk_server;
+
+typedef struct xk_server_opts {
+    double hbm_budget_bytes;          /* admission budget; 0 = 120e9 */
+    double epoch_pairs;               /* ray x screen pairs per epoch; 0 = 2e10 */
+    int max_active;                   /* admitted requests at once; 0 = 64 */
+    double item_pairs;                /* target pairs per work item; 0 = 4e6 */
+    int inject_alloc_failure_every;   /* testing: fail every k-th request allocation; 0 = off */
+} xk_server_opts;
+
+typedef struct xk_request {
+    xk_rays rays;       /* host pointers; ignored when rayset != 0 */
+    size_t n_rays;
+    uint64_t rayset;    /* handle from xk_server_upload_rays, 0 = use `rays` */
+    xk_pixels pixels;   /* host pointers */
+    size_t n_pix;       /* > 0 */
+    xk_field out;       /* host pointers, written before the request completes */
+    int path;           /* XK_PATH_F32PR or XK_PATH_F64 */
+} xk_request;
+
+typedef struct xk_request_stats {
+    double pairs;
+    double queue_ms;    /* submit -> admitted */
+    double plan_ms;     /* admitted -> planned (copies + planning) */
+    double run_ms;      /* planned -> result on the host */
+    double total_ms;    /* submit -> result on the host */
+    int path;           /* path actually used */
+    int epochs;         /* epochs that ran this request's items */
+    int status;
+} xk_request_stats;
+
+typedef struct xk_server_stats {
+    long long submitted, completed, failed, epochs, kernels, pending, active;
+    double pairs_done, used_bytes, peak_bytes, resident_ray_bytes;
+} xk_server_stats;
+
+int xk_server_create(xk_ctx* ctx, const xk_server_opts* opts, xk_server** out);
+
+/* Copies a ray set to the device and keeps it there for any number of
+ * requests (screens) until released; it counts against the budget. */
+int xk_server_upload_rays(xk_server* server, const xk_rays* rays, size_t n, uint64_t* handle);
+int xk_server_release_rays(xk_server* server, uint64_t handle);
+
+/* Queues a request; its host buffers must stay valid until xk_server_wait
+ * returns for the ticket. Returns at once. */
+int xk_server_submit(xk_server* server, const xk_request* req, uint64_t* ticket);
+
+/* Blocks until the request completes (timeout_ms < 0: no limit; on time-out
+ * returns XK_ERR_TIMEOUT and the ticket stays valid). Returns the request's
+ * own status (XK_ERR_BUDGET if it alone exceeds the budget, XK_ERR_SHUTDOWN if
+ * the server stopped before admitting it) and releases the ticket. */
+int xk_server_wait(xk_server* server, uint64_t ticket, double timeout_ms,
+                   xk_request_stats* stats);
+
+int xk_server_get_stats(xk_server* server, xk_server_stats* out);
+
+/* Stops admitting, finishes admitted requests, cancels pending ones. */
+void xk_server_destroy(xk_server* server);
+
 /* ---- allocation-free FP64 solve ---------------------------------------------
  *
  * No counterpart in the reference. For callers that cannot let a library

@@ -16,6 +16,15 @@
  *                      per-ray term is computed exactly as Rust computes it.
  *   oracle_plain_f64   src/gpu/fallback.rs:29-71 (kirchhoff_cpu_from_gpu_types):
  *                      f64 plain sum (no Kahan), `* inv_path`, skip < 1e-20.
+ *   oracle_kahan_ld    the same formula with the phase k*|p - r| evaluated in
+ *                      x87 extended precision (64-bit significand: |p - r| from
+ *                      exact differences, sqrtl, sinl/cosl) and everything else
+ *                      as oracle_kahan_f64. At 30 keV and 20 m k*path is 3e12
+ *                      rad, where one FP64 rounding of the phase is 4.9e-4 rad,
+ *                      so the FP64 formula itself carries ~1e-4 relative error
+ *                      on noise-like fields; this variant measures that error
+ *                      and is the reference for the FP32 phase-reduced path at
+ *                      such phases.
  *   oracle_wgsl_f32    src/gpu/shaders/kirchhoff.wgsl:56-135 + the host side in
  *                      src/gpu/kirchhoff.rs:96-297: f32 phase-reduced sum about
  *                      an f32-rounded ray centroid, naive f32 accumulation,
@@ -115,6 +124,69 @@ void oracle_kahan_f64(const double* rx, const double* ry, const double* rz,
         double o[4];
         kahan_pixel(rx, ry, rz, rnx, rny, rnz, rnl, es_re, es_im, ep_re, ep_im, energy,
                     n_rays, px[i], py[i], pz[i], o);
+        o_es_re[i] = o[0]; o_es_im[i] = o[1]; o_ep_re[i] = o[2]; o_ep_im[i] = o[3];
+    }
+}
+
+/* diffraction.rs:67-117 with an extended-precision phase. */
+static void kahan_pixel_ld(const double* rx, const double* ry, const double* rz,
+                           const double* rnx, const double* rny, const double* rnz,
+                           const double* rnl, const double* es_re, const double* es_im,
+                           const double* ep_re, const double* ep_im, const double* energy,
+                           size_t n_rays, double px, double py, double pz, double out[4]) {
+    cplx es_sum = {0.0, 0.0}, ep_sum = {0.0, 0.0};
+    cplx es_comp = {0.0, 0.0}, ep_comp = {0.0, 0.0};
+    for (size_t j = 0; j < n_rays; ++j) {
+        double dx = px - rx[j];
+        double dy = py - ry[j];
+        double dz = pz - rz[j];
+        double path = sqrt(dx * dx + dy * dy + dz * dz);
+        if (path < 1e-30) continue;
+        double ns = (rnx[j] * dx + rny[j] * dy + rnz[j] * dz) / path;
+        double k = energy[j] / ORACLE_CHBAR * 1e7;
+        long double lx = (long double)px - (long double)rx[j];
+        long double ly = (long double)py - (long double)ry[j];
+        long double lz = (long double)pz - (long double)rz[j];
+        long double phase = (long double)k * sqrtl(lx * lx + ly * ly + lz * lz);
+        cplx exp_ikr = {(double)cosl(phase), (double)sinl(phase)};
+        double obliquity = rnl[j] + ns;
+        double af = k / (4.0 * ORACLE_PI) * obliquity / path;
+        cplx i_af = {0.0 * af, 1.0 * af};
+        cplx u = c_mul(i_af, exp_ikr);
+
+        cplx es = {es_re[j], es_im[j]};
+        cplx t = c_mul(es, u);
+        cplx es_term = {t.re - es_comp.re, t.im - es_comp.im};
+        cplx es_new = {es_sum.re + es_term.re, es_sum.im + es_term.im};
+        es_comp.re = (es_new.re - es_sum.re) - es_term.re;
+        es_comp.im = (es_new.im - es_sum.im) - es_term.im;
+        es_sum = es_new;
+
+        cplx ep = {ep_re[j], ep_im[j]};
+        cplx tp = c_mul(ep, u);
+        cplx ep_term = {tp.re - ep_comp.re, tp.im - ep_comp.im};
+        cplx ep_new = {ep_sum.re + ep_term.re, ep_sum.im + ep_term.im};
+        ep_comp.re = (ep_new.re - ep_sum.re) - ep_term.re;
+        ep_comp.im = (ep_new.im - ep_sum.im) - ep_term.im;
+        ep_sum = ep_new;
+    }
+    out[0] = es_sum.re; out[1] = es_sum.im; out[2] = ep_sum.re; out[3] = ep_sum.im;
+}
+
+void oracle_kahan_ld(const double* rx, const double* ry, const double* rz,
+                     const double* rnx, const double* rny, const double* rnz,
+                     const double* rnl, const double* es_re, const double* es_im,
+                     const double* ep_re, const double* ep_im, const double* energy,
+                     size_t n_rays, const double* px, const double* py, const double* pz,
+                     size_t n_pix, double* o_es_re, double* o_es_im, double* o_ep_re,
+                     double* o_ep_im, int n_threads) {
+    set_threads(n_threads);
+    long long m = (long long)n_pix;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long long i = 0; i < m; ++i) {
+        double o[4];
+        kahan_pixel_ld(rx, ry, rz, rnx, rny, rnz, rnl, es_re, es_im, ep_re, ep_im, energy,
+                       n_rays, px[i], py[i], pz[i], o);
         o_es_re[i] = o[0]; o_es_im[i] = o[1]; o_ep_re[i] = o[2]; o_ep_im[i] = o[3];
     }
 }

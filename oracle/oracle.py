@@ -39,7 +39,7 @@ def _load():
         d = ctypes.POINTER(ctypes.c_double)
         f = ctypes.POINTER(ctypes.c_float)
         sz = ctypes.c_size_t
-        for name in ("oracle_kahan_f64", "oracle_plain_f64"):
+        for name in ("oracle_kahan_f64", "oracle_plain_f64", "oracle_kahan_ld"):
             fn = getattr(lib, name)
             fn.argtypes = [d] * 12 + [sz] + [d] * 3 + [sz] + [d] * 4 + [ctypes.c_int]
             fn.restype = None
@@ -81,6 +81,13 @@ def _run(fn_name, rays, pixels, dtype, threads):
 def kahan_f64(rays, pixels, threads: int = 0):
     """src/waves/diffraction.rs:56-117 restated (the correctness oracle)."""
     return _run("oracle_kahan_f64", rays, pixels, np.float64, threads)
+
+
+def kahan_ld(rays, pixels, threads: int = 0):
+    """kahan_f64 with the phase k*|p - r| in x87 extended precision: the
+    formula's value without FP64's phase rounding (which reaches 1e-4 rad at
+    k*path ~ 1e12)."""
+    return _run("oracle_kahan_ld", rays, pixels, np.float64, threads)
 
 
 def plain_f64(rays, pixels, threads: int = 0):

@@ -228,3 +228,19 @@ def test_phase_budget_option(sweep_ctx, oracle):
         sweep_ctx.set_option("phase_budget", 256.0)
     assert st["phase_bound_rad"] <= 32.0 + 1e-9
     assert cases.rel_l2(out, ref) < PR_TOL
+
+
+@pytest.mark.parametrize("energy,dist", [(30000.0, 20000.0), (30000.0, 100.0), (1000.0, 20000.0)])
+def test_f32pr_extreme_cells_vs_extended_oracle(ctx, oracle, energy, dist):
+    """Corners of the E <= 30 keV, d <= 20 m range, 4096 rays x 32x32 screen.
+    The FP32 phase-reduced form is compared with the extended-precision oracle;
+    the FP64 formula's own distance from it is printed beside."""
+    rays, screen, meta = synth.config2_cell(energy, dist, seed=17, n_rays=4096, grid=32)
+    rl, pl = cases.as_lists(rays, screen)
+    exact = oracle.kahan_ld(rl, pl)
+    out, st = run(ctx, rays, screen, "f32pr")
+    err = cases.rel_l2(out, exact)
+    f64_err = cases.rel_l2(oracle.kahan_f64(rl, pl), exact)
+    print(f"E={energy} d={dist}: f32pr vs exact {err:.2e}, fp64 formula vs exact {f64_err:.2e}, "
+          f"chunks={st['n_chunks']} path={st['path']}")
+    assert err < PR_TOL

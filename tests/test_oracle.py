@@ -121,3 +121,17 @@ def test_thread_count_does_not_change_results(oracle):
 def test_empty_rays_give_zero(oracle):
     out = oracle.kahan_f64([[]] * 12, [[0.0], [0.0], [1000.0]])
     assert all(o[0] == 0.0 for o in out)
+
+
+def test_extended_phase_oracle_measures_fp64_phase_rounding(oracle):
+    """oracle_kahan_ld differs from the FP64 formula only by FP64's rounding of
+    k*|p - r|: ~1e-6 at 10 keV and 1 m (5e10 rad), ~1e-4 at 24 keV and 8 m."""
+    from xrt_rs import synth
+    rays, pix = synth.config0(seed=0)
+    rl, pl = cases.as_lists(rays, pix)
+    d = cases.rel_l2(oracle.kahan_f64(rl, pl), oracle.kahan_ld(rl, pl))
+    assert 1e-8 < d < 1e-5
+    far, fpix, _ = synth.config3(seed=0, count=2, ray_range=(300, 30000), pix_range=(17, 4000))[1]
+    rl, pl = cases.as_lists(far, fpix)
+    d_far = cases.rel_l2(oracle.kahan_f64(rl, pl), oracle.kahan_ld(rl, pl))
+    assert d_far > 10 * d

@@ -9,23 +9,7 @@
 #include <cstring>
 #include <vector>
 
-#include "xk_internal.cuh"
-#include "xk_pr.cuh"
-
-struct xk_ctx {
-    int device = 0;
-    int num_sms = 0;
-    bool is_shared = false;
-    std::string name;
-    std::string last_error;
-    std::mutex mu;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    xk::F64Workspace f64ws;
-    xk::PrWorkspace prws;
-    xk::PrOptions pr_opts;
-    xk::DevBuf in_rays, in_pix, out_field;
-};
+#include "xk_ctx.cuh"
 
 namespace {
 

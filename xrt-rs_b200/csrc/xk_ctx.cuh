@@ -1,0 +1,22 @@
+// The context object behind the opaque xk_ctx handle (include/xk.h).
+#pragma once
+
+#include <string>
+
+#include "xk_internal.cuh"
+#include "xk_pr.cuh"
+
+struct xk_ctx {
+    int device = 0;
+    int num_sms = 0;
+    bool is_shared = false;
+    std::string name;
+    std::string last_error;
+    std::mutex mu;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    xk::F64Workspace f64ws;
+    xk::PrWorkspace prws;
+    xk::PrOptions pr_opts;
+    xk::DevBuf in_rays, in_pix, out_field;
+};

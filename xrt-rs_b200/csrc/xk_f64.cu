@@ -177,6 +177,30 @@ __global__ void zero_field_kernel(FieldDev out, size_t n_pix) {
 
 }  // namespace
 
+size_t f64_splits(size_t n_rays, size_t n_pix, int num_sms, size_t* rays_per_split) {
+    const size_t pix_per_cta = (size_t)kF64Threads * kF64Ppt;
+    const size_t pix_ctas = (n_pix + pix_per_cta - 1) / pix_per_cta;
+    // Aim for about 32 CTAs per SM in flight; never split below one stage.
+    const size_t want = (size_t)num_sms * 32;
+    size_t splits = (want + pix_ctas - 1) / pix_ctas;
+    size_t max_splits = (n_rays + kF64Stage - 1) / kF64Stage;
+    if (splits > max_splits) splits = max_splits;
+    if (splits > 65535) splits = 65535;
+    if (splits < 1) splits = 1;
+    size_t per = (n_rays + splits - 1) / splits;
+    per = (per + kF64Stage - 1) / kF64Stage * kF64Stage;
+    if (rays_per_split) *rays_per_split = per;
+    return per ? (n_rays + per - 1) / per : 1;
+}
+
+Status f64_reserve(size_t n_rays, size_t n_pix, int num_sms, F64Workspace& ws) {
+    if (n_rays == 0 || n_pix == 0) return Status::Ok();
+    XK_TRY(ws.rays.ensure(n_rays * sizeof(RayRec64)));
+    const size_t splits = f64_splits(n_rays, n_pix, num_sms, nullptr);
+    if (splits > 1) XK_TRY(ws.partials.ensure(splits * 4 * n_pix * sizeof(double)));
+    return Status::Ok();
+}
+
 Status f64_enqueue(const RaysDev& rays, size_t n_rays, const PixDev& pix, size_t n_pix,
                    const FieldDev& out, F64Workspace& ws, cudaStream_t stream, int num_sms,
                    LaunchReport* rep) {
@@ -194,16 +218,8 @@ Status f64_enqueue(const RaysDev& rays, size_t n_rays, const PixDev& pix, size_t
 
     const size_t pix_per_cta = (size_t)kF64Threads * kF64Ppt;
     const size_t pix_ctas = (n_pix + pix_per_cta - 1) / pix_per_cta;
-    // Aim for about 32 CTAs per SM in flight; never split below one stage.
-    const size_t want = (size_t)num_sms * 32;
-    size_t splits = (want + pix_ctas - 1) / pix_ctas;
-    size_t max_splits = (n_rays + kF64Stage - 1) / kF64Stage;
-    if (splits > max_splits) splits = max_splits;
-    if (splits > 65535) splits = 65535;
-    if (splits < 1) splits = 1;
-    size_t rays_per_split = (n_rays + splits - 1) / splits;
-    rays_per_split = (rays_per_split + kF64Stage - 1) / kF64Stage * kF64Stage;
-    splits = (n_rays + rays_per_split - 1) / rays_per_split;
+    size_t rays_per_split = 0;
+    const size_t splits = f64_splits(n_rays, n_pix, num_sms, &rays_per_split);
 
     double* partials = nullptr;
     if (splits > 1) {

@@ -41,22 +41,30 @@ struct Status {
         if (!st__.ok()) return st__;      \
     } while (0)
 
-// A growable device buffer owned by a context (never shrinks until freed).
+// A growable device buffer (never shrinks until freed). With `async_stream`
+// set it allocates and frees stream-ordered (cudaMallocAsync/cudaFreeAsync on
+// that stream), which never waits for other streams' work.
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t async_stream = nullptr;
     Status ensure(size_t want) {
         if (want <= bytes) return Status::Ok();
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
+        release();
         size_t rounded = (want + ((size_t)1 << 20) - 1) & ~(((size_t)1 << 20) - 1);
-        XK_CUDA_TRY(cudaMalloc(&ptr, rounded));
+        if (async_stream) {
+            XK_CUDA_TRY(cudaMallocAsync(&ptr, rounded, async_stream));
+        } else {
+            XK_CUDA_TRY(cudaMalloc(&ptr, rounded));
+        }
         bytes = rounded;
         return Status::Ok();
     }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            if (async_stream) cudaFreeAsync(ptr, async_stream);
+            else cudaFree(ptr);
+        }
         ptr = nullptr;
         bytes = 0;
     }
@@ -85,6 +93,13 @@ struct LaunchReport {
     int kernels = 0;
     float gpu_ms = 0.f;
 };
+
+// Ray-range splits of the FP64 path for a solve (and the rays per range).
+size_t f64_splits(size_t n_rays, size_t n_pix, int num_sms, size_t* rays_per_split);
+
+// Grows `ws` to what f64_enqueue needs for this solve, so a later enqueue
+// allocates nothing (e.g. while a CUDA graph is being captured).
+Status f64_reserve(size_t n_rays, size_t n_pix, int num_sms, F64Workspace& ws);
 
 // FP64 plain path (xk_f64.cu). All pointers are device pointers; the call
 // enqueues on `stream` and does not synchronise.

@@ -230,6 +230,7 @@ struct CellGrid {
     Frame fr;        // origin, axes, lo[] (cell-grid origin in frame coords)
     double cell[3];  // cell size per axis
     long long n[3];  // cells per axis
+    double quantum, inv_quantum;  // chunk centres are multiples of quantum (a power of two)
 };
 
 __device__ __forceinline__ void cell_of(const CellGrid& g, double x, double y, double z,
@@ -277,9 +278,15 @@ __global__ void chunk_table_kernel(const uint64_t* __restrict__ keys, const int*
         double f1 = g.fr.lo[1] + (iy + 0.5) * g.cell[1];
         double f2 = g.fr.lo[2] + (iz + 0.5) * g.cell[2];
         const Frame& fr = g.fr;
-        chunk_center[3 * c + 0] = fr.ox + f0 * fr.e1[0] + f1 * fr.e2[0] + f2 * fr.u0[0];
-        chunk_center[3 * c + 1] = fr.oy + f0 * fr.e1[1] + f1 * fr.e2[1] + f2 * fr.u0[1];
-        chunk_center[3 * c + 2] = fr.oz + f0 * fr.e1[2] + f1 * fr.e2[2] + f2 * fr.u0[2];
+        // Snapped to multiples of g.quantum (a power of two no smaller than the
+        // ulp of any coordinate in play), so that q = p - R0 is exact: at
+        // |p| ~ 2e4 mm one rounding of q is 1.8e-12 mm, 2.8e-4 rad at 30 keV.
+        const double cx = fr.ox + f0 * fr.e1[0] + f1 * fr.e2[0] + f2 * fr.u0[0];
+        const double cy = fr.oy + f0 * fr.e1[1] + f1 * fr.e2[1] + f2 * fr.u0[1];
+        const double cz = fr.oz + f0 * fr.e1[2] + f1 * fr.e2[2] + f2 * fr.u0[2];
+        chunk_center[3 * c + 0] = rint(cx * g.inv_quantum) * g.quantum;
+        chunk_center[3 * c + 1] = rint(cy * g.inv_quantum) * g.quantum;
+        chunk_center[3 * c + 2] = rint(cz * g.inv_quantum) * g.quantum;
     }
     if (i == n - 1) {
         int nc = run_id[i];
@@ -434,6 +441,29 @@ struct PackedState {
     float2 acc[kPrPpl / 2][4];
 };
 
+// Fractional part of (kt_hi + kt_lo) * |q| in turns, |q| = sqrt(qx^2+qy^2+qz^2),
+// evaluated in double-double arithmetic (error-free products by FMA, TwoSum,
+// one Newton correction of the square root).
+__device__ __forceinline__ double dd_turns(double kt_hi, double kt_lo, double qx, double qy,
+                                           double qz) {
+    const double p0 = qx * qx, p1 = qy * qy, p2 = qz * qz;
+    const double e0 = fma(qx, qx, -p0), e1 = fma(qy, qy, -p1), e2 = fma(qz, qz, -p2);
+    double s1 = p0 + p1;
+    double b1 = s1 - p0;
+    double t1 = (p0 - (s1 - b1)) + (p1 - b1);
+    double s2 = s1 + p2;
+    double b2 = s2 - s1;
+    double t2 = (s1 - (s2 - b2)) + (p2 - b2);
+    double lo = t1 + t2 + e0 + e1 + e2;
+    double hi = s2 + lo;
+    lo -= hi - s2;
+    const double r = sqrt(hi);
+    const double rl = (fma(-r, r, hi) + lo) / (2.0 * r);
+    const double ph = kt_hi * r;
+    const double pe = fma(kt_hi, r, -ph) + (kt_hi * rl + kt_lo * r);
+    return (ph - rint(ph)) + pe;
+}
+
 // Per chunk: FP64 geometry of the lane's points, written into the sweep
 // state, and the per-point phasor into shared memory.
 template <bool UNIFORM, bool FAST, class State>
@@ -468,9 +498,9 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
             qyp[i] = (float)qy;
             qzp[i] = (float)qz;
         }
-        // Base phase k|q| reduced to turns in FP64; sin/cos of the fraction.
-        double turns = sv.kt * qn;
-        float fr = (float)(turns - rint(turns));
+        // Base phase k|q| in turns, carried in double-double: k|q| reaches
+        // 1e12 rad at 30 keV and 20 m, where one FP64 rounding is 1e-4 rad.
+        float fr = (float)dd_turns(sv.kt, sv.kt_lo, qx, qy, qz);
         float sp, cp;
         sincospif(2.0f * fr, &sp, &cp);
         ws.ph[i][lane] = make_float2(-kt * sp, kt * cp);
@@ -677,11 +707,19 @@ __device__ __forceinline__ int chunk_of(const int* __restrict__ begin, int n_chu
 template <bool UNIFORM, bool FAST>
 __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, WarpShared& ws,
                              int lane) {
+    // local = (sub * groups + g) * n_tiles + t: sub-range `sub` of ray group g
+    // against tile t. Sub-items of one (g, t) add into the same slots, so a
+    // launch must never hold two of them (launches cover at most
+    // groups * n_tiles consecutive items of a solve).
     const int t = (int)(local % sv.n_tiles);
-    const int g = (int)(local / sv.n_tiles);
+    const long long rest = local / sv.n_tiles;
+    const int g = (int)(rest % sv.groups);
+    const int sub = (int)(rest / sv.groups);
     const long long n = sv.n_rays;
-    const int r0 = (int)((long long)g * n / sv.groups);
-    const int r1 = (int)((long long)(g + 1) * n / sv.groups);
+    const long long g0 = (long long)g * n / sv.groups;
+    const long long g1 = (long long)(g + 1) * n / sv.groups;
+    const int r0 = (int)(g0 + (g1 - g0) * sub / sv.subs);
+    const int r1 = (int)(g0 + (g1 - g0) * (sub + 1) / sv.subs);
     if (r0 >= r1) return true;
     const int n_chunks = *sv.n_chunks_dev;
     const int* __restrict__ cb = sv.chunk_begin;
@@ -757,7 +795,9 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
 }
 
 // Every solve in `solves` must match the kernel's variant (normal mode and
-// sweep); solves[s].item_begin is the prefix sum of the item counts.
+// sweep); solves[s].item_begin is the prefix sum of the item counts in this
+// launch, and the launch covers items [item_offset, item_offset + count) of
+// each solve.
 template <bool UNIFORM, bool FAST>
 __global__ void __launch_bounds__(kPrWarpsPerCta * 32, 3)
 pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long n_items,
@@ -792,7 +832,7 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
             else hi = mid - 1;
         }
         const PrSolve& sv = solves[lo];
-        const long long local = item - sv.item_begin;
+        const long long local = item - sv.item_begin + sv.item_offset;
         const bool ok = process_item<UNIFORM, FAST>(sv, local, wp, *wsh, lane);
         if (!ok) {
             if (lane == 0) atomicExch(err, 1);
@@ -943,6 +983,18 @@ HostLayout host_layout(int count, int sum_blocks) {
 
 int sum_blocks_for(int num_sms) { return std::min(512, std::max(1, 2 * num_sms)); }
 
+// Ray groups per tile: enough items to keep every resident warp busy, at
+// least four stages of rays per item, partial slots within 1 GiB.
+int plan_groups(int n, int n_tiles, int num_sms, const PrOptions& opt) {
+    if (opt.groups > 0) return opt.groups;
+    long long want = (long long)num_sms * 12 * opt.items_per_warp;
+    int g = (int)std::max<long long>(1, (want + n_tiles - 1) / n_tiles);
+    g = std::min(g, std::max(1, n / (4 * kPrStage)));
+    long long cap = (1LL << 30) / (32LL * n_tiles * kPrTile);
+    g = (int)std::max<long long>(1, std::min<long long>(g, cap));
+    return std::min(g, 4096);
+}
+
 }  // namespace
 
 const char* const kRouteReasons[kRouteReasonCount] = {
@@ -956,6 +1008,7 @@ const char* const kRouteReasons[kRouteReasonCount] = {
 
 Status PrWorkspace::ensure_host(size_t bytes) {
     if (bytes <= host_bytes) return Status::Ok();
+    if (host_borrowed) return Status::Err(XK_ERR_OOM, "borrowed pinned area too small");
     if (host) cudaFreeHost(host);
     host = nullptr;
     host_bytes = 0;
@@ -973,10 +1026,24 @@ void PrWorkspace::release() {
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     ev[0] = ev[1] = nullptr;
-    if (host) cudaFreeHost(host);
+    if (host && !host_borrowed) cudaFreeHost(host);
     host = nullptr;
     host_bytes = 0;
     host_err = nullptr;
+    host_borrowed = false;
+}
+
+size_t pr_plan_bytes(size_t n, size_t m, int num_sms, const PrOptions& opt) {
+    if (n == 0 || m == 0) return 0;
+    const int sum_blocks = sum_blocks_for(num_sms);
+    const int n_tiles = (int)((m + kPrTile - 1) / kPrTile);
+    const int g = plan_groups((int)n, n_tiles, num_sms, opt);
+    Arena a{nullptr, 0};
+    SolveBufs b;
+    carve(a, b, (int)n, (int)m, n_tiles, g, sum_blocks);
+    // CUB radix sort of 64-bit keys + 32-bit values and the scan need at most
+    // a few bytes per item; 16 per item plus 1 MiB bounds them.
+    return a.off + 16 * std::max(n, m) + (1u << 20) + (2u << 20);
 }
 
 Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t stream, int num_sms,
@@ -1000,17 +1067,7 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             return Status::Err(XK_ERR_INVALID, "too many rays or screen points for one solve");
         const int n = (int)in[s].n, m = (int)in[s].m;
         n_tiles[s] = (m + kPrTile - 1) / kPrTile;
-        int g = opt.groups;
-        if (g <= 0) {
-            // Enough items to keep every resident warp busy, at least four
-            // stages of rays per item, partial slots within 1 GiB.
-            long long want = (long long)num_sms * 12 * opt.items_per_warp;
-            g = (int)std::max<long long>(1, (want + n_tiles[s] - 1) / n_tiles[s]);
-            g = std::min(g, std::max(1, n / (4 * kPrStage)));
-            long long cap = (1LL << 30) / (32LL * n_tiles[s] * kPrTile);
-            g = (int)std::max<long long>(1, std::min<long long>(g, cap));
-            g = std::min(g, 4096);
-        }
+        const int g = plan_groups(n, n_tiles[s], num_sms, opt);
         groups[s] = g;
         size_t c1 = 0, c2 = 0, c3 = 0;
         XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, c1, (uint64_t*)nullptr,
@@ -1221,6 +1278,17 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             P.route_reason = 6;
             continue;
         }
+        {
+            // 2^E bounds every screen and ray coordinate; multiples of 2^(E-52)
+            // then subtract from any screen coordinate exactly.
+            double amax = 0.0;
+            for (int a = 0; a < 3; ++a)
+                amax = std::max(amax, std::max(std::max(std::fabs(I.plo[a]), std::fabs(I.phi[a])),
+                                               std::max(std::fabs(I.rlo[a]), std::fabs(I.rhi[a]))));
+            const int e = amax > 0 ? std::ilogb(amax) + 2 : -1000;
+            cg.quantum = std::ldexp(1.0, e - 52);
+            cg.inv_quantum = std::ldexp(1.0, 52 - e);
+        }
         P.phase_bound = phase_bound(k, a_max, b_max, I.d_lo);
         // |e| = |u.rho| / |q| <= b / (d_lo - b): the series reciprocal's
         // argument.
@@ -1256,12 +1324,20 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         D.tile_center = B.tile_center;
         D.partial = B.partial;
         D.item_begin = 0;
+        D.item_offset = 0;
+        D.subs = 1;
         D.n_items = (long long)n_tiles[s] * groups[s];
         D.n_rays = n;
         D.n_tiles = n_tiles[s];
         D.groups = groups[s];
         D.k = k;
-        D.kt = k / (2.0 * kPi);
+        {
+            // k/(2 pi) as a double-double, k taken as the FP64 value the
+            // reference computes (E / CHBAR * 1e7).
+            const long double kt_ld = (long double)k / (2.0L * 3.14159265358979323846264338327950288L);
+            D.kt = (double)kt_ld;
+            D.kt_lo = (double)(kt_ld - (long double)D.kt);
+        }
         D.unx = (float)I.f[11];
         D.uny = (float)I.f[12];
         D.unz = (float)I.f[13];
@@ -1275,22 +1351,63 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
     return Status::Ok();
 }
 
+Status pr_zero_partials(const PrPlan& P, cudaStream_t stream) {
+    const size_t slots = (size_t)P.n_tiles * kPrTile;
+    XK_CUDA_TRY(cudaMemsetAsync(P.dev.partial, 0, (size_t)P.groups * 4 * slots * sizeof(double),
+                                stream));
+    return Status::Ok();
+}
+
+Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, bool uniform, bool fast,
+                 unsigned long long* d_counter, int* d_err, cudaStream_t stream, int num_sms,
+                 int max_ctas_per_sm) {
+    if (n_items <= 0) return Status::Ok();
+    PrKernel kern = pr_kernel(uniform, fast);
+    XK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kPrSmemBytes));
+    int per_sm = 0;
+    XK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPrWarpsPerCta * 32,
+                                                              kPrSmemBytes));
+    per_sm = std::max(per_sm, 1);
+    if (max_ctas_per_sm > 0) per_sm = std::min(per_sm, max_ctas_per_sm);
+    long long grid = (long long)num_sms * per_sm;
+    grid = std::max<long long>(1, std::min(grid, (n_items + kPrWarpsPerCta - 1) / kPrWarpsPerCta));
+    kern<<<(unsigned)grid, kPrWarpsPerCta * 32, kPrSmemBytes, stream>>>(d_table, n_solves, n_items,
+                                                                        d_counter, d_err);
+    XK_CUDA_TRY(cudaGetLastError());
+    return Status::Ok();
+}
+
+Status pr_finalize(const PrPlan& P, cudaStream_t stream) {
+    const int slots = P.n_tiles * kPrTile;
+    finalize_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(P.dev.partial, P.tile_perm, P.groups,
+                                                             slots, P.out);
+    XK_CUDA_TRY(cudaGetLastError());
+    return Status::Ok();
+}
+
+Status pr_reserve_exec(PrWorkspace& ws, int count, int num_sms) {
+    const HostLayout HL = host_layout(count, sum_blocks_for(num_sms));
+    XK_TRY(ws.ensure_host(HL.total));
+    XK_TRY(ws.solves.ensure(std::max<size_t>(1, count) * sizeof(PrSolve)));
+    XK_TRY(ws.ctrl.ensure(256));
+    if (!ws.ev[0]) XK_CUDA_TRY(cudaEventCreate(&ws.ev[0]));
+    if (!ws.ev[1]) XK_CUDA_TRY(cudaEventCreate(&ws.ev[1]));
+    return Status::Ok();
+}
+
 Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStream_t stream,
                           int num_sms, bool time_kernels, PrExecReport* rep) {
     PrExecReport local;
     PrExecReport& R = rep ? *rep : local;
     const int count = (int)plans.size();
     const HostLayout HL = host_layout(count, sum_blocks_for(num_sms));
-    XK_TRY(ws.ensure_host(HL.total));
+    XK_TRY(pr_reserve_exec(ws, count, num_sms));
     char* hbase = static_cast<char*>(ws.host);
     PrSolve* h_tab = reinterpret_cast<PrSolve*>(hbase + HL.tab_off);
     int* h_nch = reinterpret_cast<int*>(hbase + HL.nch_off);
     ws.host_err = reinterpret_cast<int*>(hbase + HL.err_off);
     *ws.host_err = 0;
-    XK_TRY(ws.solves.ensure(std::max<size_t>(1, count) * sizeof(PrSolve)));
-    XK_TRY(ws.ctrl.ensure(256));
-    if (!ws.ev[0]) XK_CUDA_TRY(cudaEventCreate(&ws.ev[0]));
-    if (!ws.ev[1]) XK_CUDA_TRY(cudaEventCreate(&ws.ev[1]));
     unsigned long long* d_counters = reinterpret_cast<unsigned long long*>(ws.ctrl.ptr);
     int* d_err = reinterpret_cast<int*>(static_cast<char*>(ws.ctrl.ptr) + 128);
     XK_CUDA_TRY(cudaMemsetAsync(ws.ctrl.ptr, 0, 256, stream));
@@ -1313,9 +1430,7 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
             h_tab[tab++] = P.dev;
             L.items += P.dev.n_items;
             L.count++;
-            const size_t slots = (size_t)P.n_tiles * kPrTile;
-            XK_CUDA_TRY(cudaMemsetAsync(P.dev.partial, 0,
-                                        (size_t)P.groups * 4 * slots * sizeof(double), stream));
+            XK_TRY(pr_zero_partials(P, stream));
         }
         if (L.count) launches.push_back(L);
     }
@@ -1325,19 +1440,8 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
     if (time_kernels) XK_CUDA_TRY(cudaEventRecord(ws.ev[0], stream));
     int li = 0;
     for (const Launch& L : launches) {
-        PrKernel kern = pr_kernel(L.uniform, L.fast);
-        XK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kPrSmemBytes));
-        int per_sm = 0;
-        XK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPrWarpsPerCta * 32,
-                                                                  kPrSmemBytes));
-        per_sm = std::max(per_sm, 1);
-        long long grid = (long long)num_sms * per_sm;
-        grid = std::max<long long>(1, std::min(grid, (L.items + kPrWarpsPerCta - 1) / kPrWarpsPerCta));
-        kern<<<(unsigned)grid, kPrWarpsPerCta * 32, kPrSmemBytes, stream>>>(
-            reinterpret_cast<const PrSolve*>(ws.solves.ptr) + L.first, L.count, L.items,
-            d_counters + li, d_err);
-        XK_CUDA_TRY(cudaGetLastError());
+        XK_TRY(pr_launch(reinterpret_cast<const PrSolve*>(ws.solves.ptr) + L.first, L.count,
+                         L.items, L.uniform, L.fast, d_counters + li, d_err, stream, num_sms, 0));
         R.kernels += 1;
         R.n_items += L.items;
         ++li;
@@ -1346,10 +1450,7 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
     for (int s = 0; s < count; ++s) {
         PrPlan& P = plans[s];
         if (P.routed) continue;
-        const int slots = P.n_tiles * kPrTile;
-        finalize_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(P.dev.partial, P.tile_perm,
-                                                                 P.groups, slots, P.out);
-        XK_CUDA_TRY(cudaGetLastError());
+        XK_TRY(pr_finalize(P, stream));
         XK_CUDA_TRY(cudaMemcpyAsync(h_nch + s, P.dev.n_chunks_dev, sizeof(int),
                                     cudaMemcpyDeviceToHost, stream));
         R.kernels += 1;

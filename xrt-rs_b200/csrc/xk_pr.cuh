@@ -47,10 +47,13 @@ struct PrSolve {
     const double* tile_center;    // [3 * n_tiles]
     double* partial;              // [groups][4][n_tiles * kPrTile], tile-slot order
     long long item_begin;         // first global item of this solve in its launch
-    long long n_items;            // n_tiles * groups
+    long long item_offset;        // first of the solve's own items covered by the launch
+    long long n_items;            // n_tiles * groups * subs
     int n_rays, n_tiles, groups;
+    int subs;                     // sub-ranges per ray group (items per (group, tile))
     double k;                     // wavenumber [1/mm]
-    double kt;                    // k / (2 pi)
+    double kt;                    // k / (2 pi), high part
+    double kt_lo;                 // k / (2 pi), low part (double-double)
     float unx, uny, unz;          // the common normal (uniform-normal kernels)
 };
 
@@ -93,20 +96,42 @@ struct PrWorkspace {
     void* host = nullptr;  // pinned readback / upload area
     size_t host_bytes = 0;
     int* host_err = nullptr;  // error word copied back by the last execution
+    bool host_borrowed = false;  // `host` belongs to the caller: never freed here
     Status ensure_host(size_t bytes);
     void release();
+    // Stream-ordered allocation for every device buffer of this workspace.
+    void set_async(cudaStream_t s) {
+        arena.async_stream = cub_tmp.async_stream = solves.async_stream = ctrl.async_stream = s;
+    }
 };
+
+// Bytes of device memory pr_plan needs for one solve of n rays and m screen
+// points (arena and CUB scratch), for admission control.
+size_t pr_plan_bytes(size_t n, size_t m, int num_sms, const PrOptions& opt);
 
 // Plans `count` solves in one pass (three host synchronisations for the
 // whole batch). Plans reference memory in ws.arena until the next call.
 Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t stream, int num_sms,
                const PrOptions& opt, std::vector<PrPlan>& plans, int* kernels);
 
+// Allocates everything pr_execute_enqueue needs for `count` solves, so that a
+// following enqueue allocates nothing (required while capturing a graph).
+Status pr_reserve_exec(PrWorkspace& ws, int count, int num_sms);
+
 // Enqueues the sweep of every non-routed plan: per kernel variant one
 // persistent launch over all of its solves, then one finalize per solve.
 // Does not synchronise; safe to capture in a CUDA graph.
 Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStream_t stream,
                           int num_sms, bool time_kernels, PrExecReport* rep);
+
+// Pieces of the execution, for callers that schedule item ranges themselves:
+// clear a plan's partial slots; one persistent launch over a device table of
+// solves (all of one variant) covering n_items items; a plan's final reduction.
+Status pr_zero_partials(const PrPlan& P, cudaStream_t stream);
+Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, bool uniform, bool fast,
+                 unsigned long long* d_counter, int* d_err, cudaStream_t stream, int num_sms,
+                 int max_ctas_per_sm);
+Status pr_finalize(const PrPlan& P, cudaStream_t stream);
 
 // After the stream is synchronised: error flag and chunk counts.
 Status pr_execute_finish(std::vector<PrPlan>& plans, PrWorkspace& ws, PrExecReport* rep);

@@ -1,0 +1,736 @@
+// Continuous-batching Kirchhoff server.
+//
+// Requests (solves of any size) arrive from any thread. A worker thread
+// admits them while the admitted set fits an HBM budget, copies their inputs
+// (or uses a resident ray set), plans them on a high-priority planning stream
+// and slices their work items into epochs: each epoch is one persistent
+// launch over items of every admitted request — a fair share of the epoch's
+// pair budget per request — so requests that arrive while others are on the
+// GPU join the next epoch and their work runs on the device together with
+// the older requests'. Two epochs are kept in flight. When a request's last
+// items have been launched, its final reduction follows on the same stream;
+// a completion thread copies the field to the caller's buffers, frees the
+// request's memory and wakes waiters.
+//
+// Results are independent of the mix: a request's items accumulate into its
+// own slots in a fixed order (sub-ranges of a ray group in sub order, groups
+// summed in group order), whichever epoch or warp runs them.
+//
+// The reference has no server (one blocking call per solve,
+// src/gpu/kirchhoff.rs:77-83); this is the serving layer for that call.
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "xk_ctx.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct RaySet {
+    xk::DevBuf buf;
+    size_t n = 0;
+    int users = 0;
+    bool released = false;
+    xk::RaysDev view() const {
+        const double* b = static_cast<const double*>(buf.ptr);
+        return xk::RaysDev{b, b + n, b + 2 * n, b + 3 * n, b + 4 * n, b + 5 * n,
+                           b + 6 * n, b + 7 * n, b + 8 * n, b + 9 * n, b + 10 * n, b + 11 * n};
+    }
+};
+
+enum class ReqState { Pending, Admitted, Running, Computed, Done };
+
+struct Req {
+    uint64_t ticket = 0;
+    xk_request r{};
+    ReqState state = ReqState::Pending;
+    int status = XK_OK;
+    double bytes = 0.0;
+    int path = XK_PATH_F32PR;
+    bool routed = false;
+    // device state
+    xk::DevBuf mem;  // inputs (unless a ray set), screen points, output field
+    xk::PrWorkspace ws;
+    std::vector<xk::PrPlan> plans;
+    xk::PrSolveIn in{};
+    long long n_items = 0, next_item = 0, slice_cap = 0;
+    double pairs_per_item = 0.0;
+    cudaEvent_t done_ev = nullptr;
+    int epochs = 0;
+    Clock::time_point t_submit, t_admit, t_planned, t_done;
+    RaySet* rayset = nullptr;
+    void* pinned = nullptr;  // borrowed planning readback area
+};
+
+constexpr int kEpochRing = 3;
+constexpr size_t kPinnedBlock = 256 << 10;  // planning readback area of one solve
+constexpr int kVariants = 4;
+
+struct EpochSlot {
+    xk::DevBuf table;     // PrSolve entries
+    xk::DevBuf ctrl;      // counters + error word
+    xk::PrSolve* h_table = nullptr;  // pinned
+    int* h_err = nullptr;            // pinned
+    cudaEvent_t ev = nullptr;
+    bool in_flight = false;
+    std::vector<Req*> reqs;
+};
+
+}  // namespace
+
+struct xk_server {
+    xk_ctx* ctx = nullptr;
+    xk_server_opts opts{};
+    xk::PrOptions pr_opts;
+    int num_sms = 0;
+    cudaStream_t plan_stream = nullptr, exec_stream = nullptr, io_stream = nullptr,
+                 f64_stream = nullptr;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Req*> pending;
+    std::vector<Req*> active;  // admitted, not yet computed
+    std::deque<Req*> computed;  // waiting for the completion thread
+    std::unordered_map<uint64_t, Req*> reqs;
+    std::unordered_map<uint64_t, RaySet*> raysets;
+    uint64_t next_ticket = 1, next_rayset = 1;
+    double used_bytes = 0.0, peak_bytes = 0.0, ray_bytes = 0.0;
+    bool stopping = false;
+    std::thread worker, finisher;
+    EpochSlot slots[kEpochRing];
+    int next_slot = 0;
+    xk::F64Workspace f64ws;
+    std::vector<void*> pinned_free;  // planning readback areas, one per admitted request
+    std::vector<void*> pinned_all;
+    long long alloc_count = 0;
+    // statistics
+    long long submitted = 0, completed = 0, failed = 0;
+    std::atomic<long long> epochs{0}, kernels{0};
+    double pairs_done = 0.0;
+    std::string last_error;
+};
+
+namespace {
+
+// Device allocation that counts against the budget's fault injector.
+xk::Status checked_ensure(xk_server* s, xk::DevBuf& b, size_t bytes) {
+    if (s->opts.inject_alloc_failure_every > 0) {
+        long long c = ++s->alloc_count;
+        if (c % s->opts.inject_alloc_failure_every == 0)
+            return xk::Status::Err(XK_ERR_OOM, "injected allocation failure");
+    }
+    return b.ensure(bytes);
+}
+
+double request_bytes(const xk_server* s, const xk_request& r, size_t n_rays) {
+    double b = 7.0 * 8.0 * (double)r.n_pix;                  // screen points + output
+    if (r.rayset == 0) b += 12.0 * 8.0 * (double)r.n_rays;   // ray inputs
+    if (r.path == XK_PATH_F32PR)
+        b += (double)xk::pr_plan_bytes(n_rays, r.n_pix, s->num_sms, s->pr_opts);
+    else
+        b += 128.0 * (double)n_rays + 64.0 * (double)r.n_pix;  // FP64 scratch (packed rays)
+    return b;
+}
+
+void finish_request(xk_server* s, Req* q, int status) {
+    // Caller holds s->mu.
+    q->status = status;
+    q->state = ReqState::Done;
+    q->t_done = Clock::now();
+    if (status == XK_OK) {
+        s->completed++;
+        s->pairs_done += (double)q->in.n * (double)q->in.m;
+    } else {
+        s->failed++;
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+}
+
+// Copies inputs, plans (FP32-PR) or enqueues the FP64 path. Runs on the worker.
+xk::Status setup_request(xk_server* s, Req* q) {
+    const xk_request& r = q->r;
+    const size_t n = q->rayset ? q->rayset->n : r.n_rays;
+    const size_t m = r.n_pix;
+    q->mem.async_stream = s->io_stream;
+    const size_t doubles = (q->rayset ? 0 : 12 * n) + 7 * m;
+    XK_TRY(checked_ensure(s, q->mem, std::max<size_t>(doubles, 1) * sizeof(double)));
+    double* cur = q->mem.as<double>();
+    if (q->rayset) {
+        q->in.rays = q->rayset->view();
+    } else {
+        const double* src[12] = {r.rays.x, r.rays.y, r.rays.z, r.rays.nx, r.rays.ny, r.rays.nz,
+                                 r.rays.nl, r.rays.es_re, r.rays.es_im, r.rays.ep_re,
+                                 r.rays.ep_im, r.rays.energy};
+        const double** dst = reinterpret_cast<const double**>(&q->in.rays);
+        for (int f = 0; f < 12; ++f) {
+            dst[f] = cur;
+            if (n) XK_CUDA_TRY(cudaMemcpyAsync(cur, src[f], n * 8, cudaMemcpyHostToDevice, s->io_stream));
+            cur += n;
+        }
+    }
+    const double* psrc[3] = {r.pixels.x, r.pixels.y, r.pixels.z};
+    const double** pdst = reinterpret_cast<const double**>(&q->in.pix);
+    for (int f = 0; f < 3; ++f) {
+        pdst[f] = cur;
+        XK_CUDA_TRY(cudaMemcpyAsync(cur, psrc[f], m * 8, cudaMemcpyHostToDevice, s->io_stream));
+        cur += m;
+    }
+    double** odst = reinterpret_cast<double**>(&q->in.out);
+    for (int f = 0; f < 4; ++f) {
+        odst[f] = cur;
+        cur += m;
+    }
+    q->in.n = n;
+    q->in.m = m;
+    // Planning reads the inputs: order the planning stream after the copies.
+    cudaEvent_t copied;
+    XK_CUDA_TRY(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+    XK_CUDA_TRY(cudaEventRecord(copied, s->io_stream));
+    XK_CUDA_TRY(cudaStreamWaitEvent(s->plan_stream, copied, 0));
+    cudaEventDestroy(copied);
+
+    XK_CUDA_TRY(cudaEventCreateWithFlags(&q->done_ev, cudaEventDisableTiming));
+    if (q->path == XK_PATH_F32PR) {
+        q->ws.set_async(s->plan_stream);
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            if (s->pinned_free.empty()) return xk::Status::Err(XK_ERR_OOM, "no planning area free");
+            q->pinned = s->pinned_free.back();
+            s->pinned_free.pop_back();
+        }
+        q->ws.host = q->pinned;
+        q->ws.host_bytes = kPinnedBlock;
+        q->ws.host_borrowed = true;
+        int nk = 0;
+        XK_TRY(xk::pr_plan(&q->in, 1, q->ws, s->plan_stream, s->num_sms, s->pr_opts, q->plans, &nk));
+        s->kernels += nk;
+        xk::PrPlan& P = q->plans[0];
+        q->routed = P.routed;
+        if (!P.routed) {
+            // Slice every ray group into sub-ranges of about item_pairs pairs.
+            const double rays_per_group = (double)n / P.groups;
+            int subs = (int)std::ceil(rays_per_group * xk::kPrTile / s->opts.item_pairs);
+            subs = std::max(1, std::min(subs, std::max(1, (int)(rays_per_group / xk::kPrStage))));
+            P.dev.subs = subs;
+            P.dev.n_items = (long long)P.n_tiles * P.groups * subs;
+            q->n_items = P.dev.n_items;
+            q->slice_cap = (long long)P.n_tiles * P.groups;
+            q->pairs_per_item = rays_per_group / subs * xk::kPrTile;
+            XK_TRY(xk::pr_zero_partials(P, s->plan_stream));
+            // The execution stream must see the plan and the cleared slots.
+            cudaEvent_t planned;
+            XK_CUDA_TRY(cudaEventCreateWithFlags(&planned, cudaEventDisableTiming));
+            XK_CUDA_TRY(cudaEventRecord(planned, s->plan_stream));
+            XK_CUDA_TRY(cudaStreamWaitEvent(s->exec_stream, planned, 0));
+            cudaEventDestroy(planned);
+            return xk::Status::Ok();
+        }
+    }
+    // FP64 path (requested, or routed by the planner): one launch on its own stream.
+    q->routed = true;
+    cudaEvent_t ready;
+    XK_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    XK_CUDA_TRY(cudaEventRecord(ready, s->plan_stream));
+    XK_CUDA_TRY(cudaStreamWaitEvent(s->f64_stream, ready, 0));
+    cudaEventDestroy(ready);
+    xk::LaunchReport rep;
+    XK_TRY(xk::f64_enqueue(q->in.rays, n, q->in.pix, m, q->in.out, s->f64ws, s->f64_stream,
+                           s->num_sms, &rep));
+    s->kernels += rep.kernels;
+    XK_CUDA_TRY(cudaEventRecord(q->done_ev, s->f64_stream));
+    return xk::Status::Ok();
+}
+
+// Waits for an epoch slot's launch, checks its error word, frees the slot.
+void retire_slot(xk_server* s, EpochSlot& e) {
+    if (!e.in_flight) return;
+    cudaEventSynchronize(e.ev);
+    e.in_flight = false;
+    if (*e.h_err != 0) {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->last_error = "persistent kernel: a bounded wait for a ray stage ran out";
+        for (Req* q : e.reqs)
+            if (q->state != ReqState::Done) q->status = XK_ERR_TIMEOUT;
+    }
+    e.reqs.clear();
+}
+
+// Builds and launches one epoch over the admitted FP32-PR requests.
+xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
+    EpochSlot& e = s->slots[s->next_slot];
+    s->next_slot = (s->next_slot + 1) % kEpochRing;
+    retire_slot(s, e);
+
+    const double budget = s->opts.epoch_pairs;
+    const double share = budget / std::max<size_t>(1, runnable.size());
+    struct Take {
+        Req* q;
+        long long first, count;
+    };
+    std::vector<Take> takes;
+    for (Req* q : runnable) {
+        long long quota = (long long)std::max(1.0, std::floor(share / std::max(1.0, q->pairs_per_item)));
+        quota = std::min(quota, q->slice_cap);
+        quota = std::min(quota, q->n_items - q->next_item);
+        if (quota <= 0) continue;
+        takes.push_back({q, q->next_item, quota});
+    }
+    if (takes.empty()) return xk::Status::Ok();
+
+    // One table, grouped by kernel variant.
+    int tab = 0;
+    long long counts[kVariants] = {0, 0, 0, 0};
+    int first[kVariants] = {0, 0, 0, 0}, nsol[kVariants] = {0, 0, 0, 0};
+    for (int v = 0; v < kVariants; ++v) {
+        const bool uniform = (v & 1) != 0, fast = (v & 2) != 0;
+        first[v] = tab;
+        for (const Take& t : takes) {
+            xk::PrPlan& P = t.q->plans[0];
+            if (P.uniform_normal != uniform || P.fast != fast) continue;
+            xk::PrSolve d = P.dev;
+            d.item_begin = counts[v];
+            d.item_offset = t.first;
+            e.h_table[tab++] = d;
+            counts[v] += t.count;
+            nsol[v]++;
+        }
+    }
+    XK_CUDA_TRY(cudaMemcpyAsync(e.table.ptr, e.h_table, tab * sizeof(xk::PrSolve),
+                                cudaMemcpyHostToDevice, s->exec_stream));
+    XK_CUDA_TRY(cudaMemsetAsync(e.ctrl.ptr, 0, 256, s->exec_stream));
+    unsigned long long* counters = e.ctrl.as<unsigned long long>();
+    int* d_err = reinterpret_cast<int*>(e.ctrl.as<char>() + 128);
+    for (int v = 0; v < kVariants; ++v) {
+        if (!nsol[v]) continue;
+        XK_TRY(xk::pr_launch(e.table.as<xk::PrSolve>() + first[v], nsol[v], counts[v], (v & 1) != 0,
+                             (v & 2) != 0, counters + v, d_err, s->exec_stream, s->num_sms, 0));
+        s->kernels++;
+    }
+    XK_CUDA_TRY(cudaMemcpyAsync(e.h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s->exec_stream));
+    for (const Take& t : takes) {
+        t.q->next_item += t.count;
+        t.q->epochs++;
+        e.reqs.push_back(t.q);
+        if (t.q->next_item >= t.q->n_items) {
+            XK_TRY(xk::pr_finalize(t.q->plans[0], s->exec_stream));
+            s->kernels++;
+            XK_CUDA_TRY(cudaEventRecord(t.q->done_ev, s->exec_stream));
+        }
+    }
+    XK_CUDA_TRY(cudaEventRecord(e.ev, s->exec_stream));
+    e.in_flight = true;
+    s->epochs++;
+    return xk::Status::Ok();
+}
+
+void release_request_memory(xk_server* s, Req* q) {
+    q->ws.release();
+    q->mem.release();
+    if (q->done_ev) cudaEventDestroy(q->done_ev);
+    q->done_ev = nullptr;
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (q->pinned) s->pinned_free.push_back(q->pinned);
+    q->pinned = nullptr;
+    s->used_bytes -= q->bytes;
+    if (q->rayset) {
+        q->rayset->users--;
+        if (q->rayset->released && q->rayset->users == 0) {
+            s->ray_bytes -= 96.0 * q->rayset->n;
+            s->used_bytes -= 96.0 * q->rayset->n;
+            q->rayset->buf.release();
+            delete q->rayset;
+        }
+        q->rayset = nullptr;
+    }
+}
+
+void worker_loop(xk_server* s) {
+    cudaSetDevice(s->ctx->device);
+    // Plans of requests admitted in this turn, ordered by admission.
+    while (true) {
+        std::vector<Req*> admitted;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            auto idle = [&] {
+                if (s->stopping) return true;
+                if (!s->pending.empty() && (int)s->active.size() < s->opts.max_active) return true;
+                for (Req* q : s->active)
+                    if (q->state == ReqState::Running && q->next_item < q->n_items) return true;
+                return false;
+            };
+            if (!idle()) s->cv_work.wait_for(lock, std::chrono::milliseconds(2), idle);
+            if (s->stopping && s->pending.empty() && s->active.empty()) break;
+            if (s->stopping) {
+                // Cancel what has not started.
+                while (!s->pending.empty()) {
+                    Req* q = s->pending.front();
+                    s->pending.pop_front();
+                    finish_request(s, q, XK_ERR_SHUTDOWN);
+                }
+            }
+            // Admission: FIFO while the budget and the slot count allow.
+            while (!s->pending.empty() && (int)s->active.size() < s->opts.max_active) {
+                Req* q = s->pending.front();
+                if (s->used_bytes + q->bytes > s->opts.hbm_budget_bytes && !s->active.empty()) break;
+                s->pending.pop_front();
+                if (q->bytes > s->opts.hbm_budget_bytes) {
+                    finish_request(s, q, XK_ERR_BUDGET);
+                    continue;
+                }
+                s->used_bytes += q->bytes;
+                s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
+                q->state = ReqState::Admitted;
+                q->t_admit = Clock::now();
+                s->active.push_back(q);
+                admitted.push_back(q);
+            }
+        }
+        for (Req* q : admitted) {
+            xk::Status st = setup_request(s, q);
+            q->t_planned = Clock::now();
+            std::lock_guard<std::mutex> lock(s->mu);
+            if (!st.ok()) {
+                s->last_error = st.msg;
+                cudaGetLastError();
+                q->status = st.code;
+                q->state = ReqState::Computed;
+                s->active.erase(std::find(s->active.begin(), s->active.end(), q));
+                s->computed.push_back(q);
+                s->cv_work.notify_all();
+                continue;
+            }
+            if (q->routed) {
+                q->state = ReqState::Computed;
+                s->active.erase(std::find(s->active.begin(), s->active.end(), q));
+                s->computed.push_back(q);
+                s->cv_work.notify_all();
+            } else {
+                q->state = ReqState::Running;
+            }
+        }
+        std::vector<Req*> runnable;
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            for (Req* q : s->active)
+                if (q->state == ReqState::Running && q->next_item < q->n_items) runnable.push_back(q);
+        }
+        if (runnable.empty()) continue;
+        xk::Status st = run_epoch(s, runnable);
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (!st.ok()) s->last_error = st.msg;
+        for (Req* q : runnable) {
+            if (q->next_item >= q->n_items || !st.ok()) {
+                if (!st.ok()) q->status = st.code;
+                q->state = ReqState::Computed;
+                s->active.erase(std::find(s->active.begin(), s->active.end(), q));
+                s->computed.push_back(q);
+            }
+        }
+        s->cv_work.notify_all();
+    }
+    for (EpochSlot& e : s->slots) retire_slot(s, e);
+}
+
+void finisher_loop(xk_server* s) {
+    cudaSetDevice(s->ctx->device);
+    while (true) {
+        Req* q = nullptr;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            s->cv_work.wait_for(lock, std::chrono::milliseconds(2),
+                                [&] { return !s->computed.empty() || s->stopping; });
+            if (s->computed.empty()) {
+                if (s->stopping && s->active.empty() && s->pending.empty()) break;
+                continue;
+            }
+            q = s->computed.front();
+            s->computed.pop_front();
+        }
+        int status = q->status;
+        if (q->done_ev) {
+            cudaError_t e = cudaEventSynchronize(q->done_ev);
+            if (e != cudaSuccess && status == XK_OK) status = XK_ERR_CUDA;
+        }
+        if (status == XK_OK && q->in.m) {
+            const size_t bytes = q->in.m * sizeof(double);
+            const xk_field& h = q->r.out;
+            double* dst[4] = {h.es_re, h.es_im, h.ep_re, h.ep_im};
+            const double* src[4] = {q->in.out.es_re, q->in.out.es_im, q->in.out.ep_re, q->in.out.ep_im};
+            for (int f = 0; f < 4; ++f)
+                if (cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyDeviceToHost, s->io_stream) != cudaSuccess)
+                    status = XK_ERR_CUDA;
+            if (cudaStreamSynchronize(s->io_stream) != cudaSuccess) status = XK_ERR_CUDA;
+        }
+        release_request_memory(s, q);
+        std::lock_guard<std::mutex> lock(s->mu);
+        finish_request(s, q, status);
+    }
+}
+
+void destroy_server(xk_server* s) {
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stopping = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    if (s->finisher.joinable()) s->finisher.join();
+    cudaSetDevice(s->ctx->device);
+    for (EpochSlot& e : s->slots) {
+        e.table.release();
+        e.ctrl.release();
+        if (e.ev) cudaEventDestroy(e.ev);
+        if (e.h_table) cudaFreeHost(e.h_table);
+        if (e.h_err) cudaFreeHost(e.h_err);
+    }
+    for (auto& kv : s->reqs) delete kv.second;
+    for (void* p : s->pinned_all) cudaFreeHost(p);
+    for (auto& kv : s->raysets) {
+        kv.second->buf.release();
+        delete kv.second;
+    }
+    s->f64ws.rays.release();
+    s->f64ws.partials.release();
+    for (cudaStream_t st : {s->plan_stream, s->exec_stream, s->io_stream, s->f64_stream})
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    delete s;
+}
+
+xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** out) {
+    xk_server* s = new xk_server();
+    *out = s;
+    s->ctx = ctx;
+    s->num_sms = ctx->num_sms;
+    if (opts) s->opts = *opts;
+    if (s->opts.hbm_budget_bytes <= 0) s->opts.hbm_budget_bytes = 120e9;
+    if (s->opts.epoch_pairs <= 0) s->opts.epoch_pairs = 2e10;
+    if (s->opts.max_active <= 0) s->opts.max_active = 64;
+    if (s->opts.item_pairs <= 0) s->opts.item_pairs = 4e6;
+    s->pr_opts = ctx->pr_opts;
+    // Keep freed stream-ordered memory in the pool instead of returning it to
+    // the driver at every synchronisation.
+    cudaMemPool_t pool;
+    XK_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+    uint64_t threshold = UINT64_MAX;
+    XK_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    int lo = 0, hi = 0;
+    XK_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->plan_stream, cudaStreamNonBlocking, hi));
+    XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->exec_stream, cudaStreamNonBlocking, lo));
+    XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->io_stream, cudaStreamNonBlocking, hi));
+    XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->f64_stream, cudaStreamNonBlocking, lo));
+    for (EpochSlot& e : s->slots) {
+        XK_TRY(e.table.ensure(kVariants * (size_t)std::max(1, s->opts.max_active) * sizeof(xk::PrSolve)));
+        XK_TRY(e.ctrl.ensure(256));
+        XK_CUDA_TRY(cudaMallocHost(&e.h_table,
+                                   kVariants * (size_t)std::max(1, s->opts.max_active) * sizeof(xk::PrSolve)));
+        XK_CUDA_TRY(cudaMallocHost(&e.h_err, 64));
+        *e.h_err = 0;
+        XK_CUDA_TRY(cudaEventCreateWithFlags(&e.ev, cudaEventDisableTiming));
+    }
+    for (int i = 0; i < s->opts.max_active; ++i) {
+        void* p = nullptr;
+        XK_CUDA_TRY(cudaMallocHost(&p, kPinnedBlock));
+        s->pinned_all.push_back(p);
+        s->pinned_free.push_back(p);
+    }
+    s->f64ws.rays.async_stream = s->f64_stream;
+    s->f64ws.partials.async_stream = s->f64_stream;
+    s->worker = std::thread(worker_loop, s);
+    s->finisher = std::thread(finisher_loop, s);
+    return xk::Status::Ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+int xk_server_create(xk_ctx* ctx, const xk_server_opts* opts, xk_server** out) {
+    if (!ctx || !out) return XK_ERR_INVALID;
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    xk_server* s = nullptr;
+    xk::Status st = create_server(ctx, opts, &s);
+    if (!st.ok()) {
+        ctx->last_error = st.msg;
+        if (s) destroy_server(s);
+        return st.code;
+    }
+    *out = s;
+    return XK_OK;
+}
+
+void xk_server_destroy(xk_server* server) {
+    if (server) destroy_server(server);
+}
+
+int xk_server_upload_rays(xk_server* s, const xk_rays* rays, size_t n, uint64_t* handle) {
+    if (!s || !rays || !handle || n == 0) return XK_ERR_INVALID;
+    if (!rays->x || !rays->y || !rays->z || !rays->nx || !rays->ny || !rays->nz || !rays->nl ||
+        !rays->es_re || !rays->es_im || !rays->ep_re || !rays->ep_im || !rays->energy)
+        return XK_ERR_INVALID;
+    const double bytes = 96.0 * (double)n;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->used_bytes + bytes > s->opts.hbm_budget_bytes) return XK_ERR_BUDGET;
+        s->used_bytes += bytes;
+        s->ray_bytes += bytes;
+        s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
+    }
+    cudaSetDevice(s->ctx->device);
+    RaySet* rs = new RaySet();
+    rs->n = n;
+    const double* src[12] = {rays->x, rays->y, rays->z, rays->nx, rays->ny, rays->nz, rays->nl,
+                             rays->es_re, rays->es_im, rays->ep_re, rays->ep_im, rays->energy};
+    int rc = XK_OK;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) rc = XK_ERR_CUDA;
+    if (rc == XK_OK && !rs->buf.ensure(12 * n * sizeof(double)).ok()) rc = XK_ERR_OOM;
+    for (int f = 0; f < 12 && rc == XK_OK; ++f)
+        if (cudaMemcpyAsync(rs->buf.as<double>() + f * n, src[f], n * 8, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess)
+            rc = XK_ERR_CUDA;
+    if (st) {
+        if (cudaStreamSynchronize(st) != cudaSuccess && rc == XK_OK) rc = XK_ERR_CUDA;
+        cudaStreamDestroy(st);
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (rc != XK_OK) {
+        s->used_bytes -= bytes;
+        s->ray_bytes -= bytes;
+        rs->buf.release();
+        delete rs;
+        return rc;
+    }
+    *handle = s->next_rayset++;
+    s->raysets[*handle] = rs;
+    return XK_OK;
+}
+
+int xk_server_release_rays(xk_server* s, uint64_t handle) {
+    if (!s) return XK_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->raysets.find(handle);
+    if (it == s->raysets.end()) return XK_ERR_NOT_FOUND;
+    RaySet* rs = it->second;
+    s->raysets.erase(it);
+    rs->released = true;
+    if (rs->users == 0) {
+        s->ray_bytes -= 96.0 * rs->n;
+        s->used_bytes -= 96.0 * rs->n;
+        rs->buf.release();
+        delete rs;
+    }
+    return XK_OK;
+}
+
+int xk_server_submit(xk_server* s, const xk_request* req, uint64_t* ticket) {
+    if (!s || !req || !ticket) return XK_ERR_INVALID;
+    if (req->path != XK_PATH_F64 && req->path != XK_PATH_F32PR) return XK_ERR_INVALID;
+    const xk_pixels& p = req->pixels;
+    const xk_field& f = req->out;
+    if (req->n_pix == 0 || !p.x || !p.y || !p.z || !f.es_re || !f.es_im || !f.ep_re || !f.ep_im)
+        return XK_ERR_INVALID;
+    Req* q = new Req();
+    q->r = *req;
+    q->path = req->path;
+    q->t_submit = Clock::now();
+    std::lock_guard<std::mutex> lock(s->mu);
+    size_t n = req->n_rays;
+    if (req->rayset) {
+        auto it = s->raysets.find(req->rayset);
+        if (it == s->raysets.end()) {
+            delete q;
+            return XK_ERR_NOT_FOUND;
+        }
+        q->rayset = it->second;
+        q->rayset->users++;
+        n = q->rayset->n;
+    } else if (n && (!req->rays.x || !req->rays.y || !req->rays.z || !req->rays.nx ||
+                     !req->rays.ny || !req->rays.nz || !req->rays.nl || !req->rays.es_re ||
+                     !req->rays.es_im || !req->rays.ep_re || !req->rays.ep_im ||
+                     !req->rays.energy)) {
+        delete q;
+        return XK_ERR_INVALID;
+    }
+    if (s->stopping) {
+        if (q->rayset) q->rayset->users--;
+        delete q;
+        return XK_ERR_SHUTDOWN;
+    }
+    q->bytes = request_bytes(s, *req, n);
+    q->ticket = s->next_ticket++;
+    s->reqs[q->ticket] = q;
+    s->pending.push_back(q);
+    s->submitted++;
+    *ticket = q->ticket;
+    s->cv_work.notify_all();
+    return XK_OK;
+}
+
+int xk_server_wait(xk_server* s, uint64_t ticket, double timeout_ms, xk_request_stats* stats) {
+    if (!s) return XK_ERR_INVALID;
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return XK_ERR_NOT_FOUND;
+    Req* q = it->second;
+    auto done = [&] { return q->state == ReqState::Done; };
+    if (timeout_ms < 0) {
+        s->cv_done.wait(lock, done);
+    } else if (!s->cv_done.wait_for(lock, std::chrono::duration<double, std::milli>(timeout_ms), done)) {
+        return XK_ERR_TIMEOUT;
+    }
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->pairs = (double)q->in.n * (double)q->in.m;
+        stats->status = q->status;
+        stats->path = q->routed ? XK_PATH_F64 : XK_PATH_F32PR;
+        stats->epochs = q->epochs;
+        if (q->t_admit.time_since_epoch().count()) {
+            stats->queue_ms = ms_between(q->t_submit, q->t_admit);
+            stats->plan_ms = ms_between(q->t_admit, q->t_planned);
+            stats->run_ms = ms_between(q->t_planned, q->t_done);
+        }
+        stats->total_ms = ms_between(q->t_submit, q->t_done);
+    }
+    const int status = q->status;
+    s->reqs.erase(it);
+    delete q;
+    return status;
+}
+
+int xk_server_get_stats(xk_server* s, xk_server_stats* out) {
+    if (!s || !out) return XK_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    std::memset(out, 0, sizeof(*out));
+    out->submitted = s->submitted;
+    out->completed = s->completed;
+    out->failed = s->failed;
+    out->epochs = s->epochs.load();
+    out->kernels = s->kernels.load();
+    out->pending = (long long)s->pending.size();
+    out->active = (long long)s->active.size();
+    out->pairs_done = s->pairs_done;
+    out->used_bytes = s->used_bytes;
+    out->peak_bytes = s->peak_bytes;
+    out->resident_ray_bytes = s->ray_bytes;
+    return XK_OK;
+}
+
+}  // extern "C"

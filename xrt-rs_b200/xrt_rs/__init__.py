@@ -26,7 +26,7 @@ from ._lib import XkError, XK_PATH_F64, XK_PATH_F32PR  # noqa: F401
 __all__ = [
     "diffraction_integral_rs", "diffraction_integral", "diffraction_integral_device",
     "GpuContext", "kirchhoff_gpu", "kirchhoff_auto", "GPU_RAY_DTYPE", "GPU_PIXEL_DTYPE",
-    "XkError", "XK_PATH_F64", "XK_PATH_F32PR", "RAY_FIELDS", "PIXEL_FIELDS",
+    "XkError", "XK_PATH_F64", "XK_PATH_F32PR", "RAY_FIELDS", "PIXEL_FIELDS", "Batch",
 ]
 
 RAY_FIELDS = ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re", "ep_im", "energy")
@@ -206,6 +206,99 @@ def diffraction_integral_device(rays, pixels, out, path="f32pr", ctx=None, strea
                                             ctypes.byref(xf), _path(path), s, ctypes.byref(st))
     _lib.check(rc, ctx.handle)
     return st.to_dict()
+
+
+class Batch:
+    """Many independent solves in one persistent launch (xk_batch_*).
+
+    ``solves`` is a sequence of (rays, pixels) pairs in the layout
+    ``diffraction_integral`` takes. The inputs are copied to the device and
+    planned once; ``run()`` replays the captured launch sequence and returns
+    one (es_re, es_im, ep_re, ep_im) tuple per solve.
+    """
+
+    def __init__(self, solves, path="f32pr", ctx=None, graph=True, device_outputs=None):
+        """With ``device_outputs`` (one 4-tuple of device tensors per solve),
+        every array in ``solves`` must be a device tensor (``data_ptr()``) and
+        results stay on the device."""
+        self._ctx = _require_ctx(ctx)
+        lib = _lib.load()
+        self._keep = []
+        self.outputs = []
+        arr = (_lib.XkSolve * max(1, len(solves)))()
+        if device_outputs is not None:
+            dp = ctypes.POINTER(ctypes.c_double)
+
+            def cast(t):
+                return ctypes.cast(ctypes.c_void_p(int(t.data_ptr())), dp)
+
+            for i, ((rays, pixels), outs) in enumerate(zip(solves, device_outputs)):
+                if isinstance(rays, dict):
+                    rays = [rays[k] for k in RAY_FIELDS]
+                if isinstance(pixels, dict):
+                    pixels = [pixels[k] for k in PIXEL_FIELDS]
+                arr[i].rays = _lib.XkRays(*[cast(a) for a in rays])
+                arr[i].n_rays = int(rays[0].numel())
+                arr[i].pixels = _lib.XkPixels(*[cast(a) for a in pixels])
+                arr[i].n_pix = int(pixels[0].numel())
+                arr[i].out = _lib.XkField(*[cast(a) for a in outs])
+                self.outputs.append(tuple(outs))
+            flags = _lib.XK_BATCH_DEVICE | (0 if graph else _lib.XK_BATCH_NO_GRAPH)
+            h = ctypes.c_void_p()
+            rc = lib.xk_batch_create(self._ctx.handle, arr, len(solves), _path(path), flags,
+                                     ctypes.byref(h))
+            _lib.check(rc, self._ctx.handle)
+            self._arr = arr
+            self._h = h
+            self.n = len(solves)
+            return
+        for i, (rays, pixels) in enumerate(solves):
+            if isinstance(rays, dict):
+                rays = [rays[k] for k in RAY_FIELDS]
+            if isinstance(pixels, dict):
+                pixels = [pixels[k] for k in PIXEL_FIELDS]
+            r = [_f64(a) for a in rays]
+            p = [_f64(a) for a in pixels]
+            _check_lengths([("ray_" + n, len(a)) for n, a in zip(RAY_FIELDS, r)])
+            _check_lengths([("pix_" + n, len(a)) for n, a in zip(PIXEL_FIELDS, p)])
+            o = [np.zeros(len(p[0]), dtype=np.float64) for _ in range(4)]
+            self._keep += r + p
+            self.outputs.append(tuple(o))
+            arr[i].rays = _lib.XkRays(*[_ptr(a) for a in r])
+            arr[i].n_rays = len(r[0])
+            arr[i].pixels = _lib.XkPixels(*[_ptr(a) for a in p])
+            arr[i].n_pix = len(p[0])
+            arr[i].out = _lib.XkField(*[_ptr(a) for a in o])
+        self._arr = arr
+        flags = 0 if graph else _lib.XK_BATCH_NO_GRAPH
+        h = ctypes.c_void_p()
+        rc = lib.xk_batch_create(self._ctx.handle, arr, len(solves), _path(path), flags,
+                                 ctypes.byref(h))
+        _lib.check(rc, self._ctx.handle)
+        self._h = h
+        self.n = len(solves)
+
+    def run(self):
+        st = _lib.XkBatchStats()
+        _lib.check(_lib.load().xk_batch_run(self._h, ctypes.byref(st)), self._ctx.handle)
+        self.stats = st.to_dict()
+        return self.outputs
+
+    def plan(self, i):
+        pl = _lib.XkSolvePlan()
+        _lib.check(_lib.load().xk_batch_solve_plan(self._h, i, ctypes.byref(pl)))
+        return pl.to_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().xk_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _as_records(a, dtype):

@@ -74,6 +74,66 @@ class XkStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class XkSolve(ctypes.Structure):
+    _fields_ = [("rays", XkRays), ("n_rays", ctypes.c_size_t), ("pixels", XkPixels),
+                ("n_pix", ctypes.c_size_t), ("out", XkField)]
+
+
+class XkBatchStats(ctypes.Structure):
+    _fields_ = [
+        ("pairs", ctypes.c_double), ("plan_ms", ctypes.c_double), ("exec_ms", ctypes.c_double),
+        ("wall_ms", ctypes.c_double), ("n_solves", ctypes.c_int), ("routed_f64", ctypes.c_int),
+        ("kernels", ctypes.c_int), ("graph", ctypes.c_int), ("n_items", ctypes.c_longlong),
+    ]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class XkSolvePlan(ctypes.Structure):
+    _fields_ = [("path", ctypes.c_int), ("routed_reason", ctypes.c_int), ("n_tiles", ctypes.c_int),
+                ("n_chunks", ctypes.c_int), ("groups", ctypes.c_int), ("sweep", ctypes.c_int),
+                ("phase_bound_rad", ctypes.c_double)]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+XK_BATCH_DEVICE = 1
+XK_BATCH_NO_GRAPH = 2
+
+
+class XkServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_double), ("epoch_pairs", ctypes.c_double),
+                ("max_active", ctypes.c_int), ("item_pairs", ctypes.c_double),
+                ("inject_alloc_failure_every", ctypes.c_int)]
+
+
+class XkRequest(ctypes.Structure):
+    _fields_ = [("rays", XkRays), ("n_rays", ctypes.c_size_t), ("rayset", ctypes.c_uint64),
+                ("pixels", XkPixels), ("n_pix", ctypes.c_size_t), ("out", XkField),
+                ("path", ctypes.c_int)]
+
+
+class XkRequestStats(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("plan_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double), ("path", ctypes.c_int), ("epochs", ctypes.c_int),
+                ("status", ctypes.c_int)]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class XkServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_longlong) for n in
+                ("submitted", "completed", "failed", "epochs", "kernels", "pending", "active")] + \
+               [(n, ctypes.c_double) for n in
+                ("pairs_done", "used_bytes", "peak_bytes", "resident_ray_bytes")]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
 # Every entry point include/xk.h declares, with its ctypes signature.
 _SIGNATURES = {
     "xk_init": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
@@ -98,6 +158,23 @@ _SIGNATURES = {
     "xk_diffraction_f64_noalloc": (ctypes.c_int, [
         ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels), ctypes.c_size_t,
         ctypes.POINTER(XkField), ctypes.c_void_p]),
+    "xk_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkSolve), ctypes.c_size_t,
+                                        ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "xk_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkBatchStats)]),
+    "xk_batch_solve_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t,
+                                            ctypes.POINTER(XkSolvePlan)]),
+    "xk_batch_destroy": (None, [ctypes.c_void_p]),
+    "xk_server_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkServerOpts),
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "xk_server_upload_rays": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkRays),
+                                              ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]),
+    "xk_server_release_rays": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "xk_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkRequest),
+                                         ctypes.POINTER(ctypes.c_uint64)]),
+    "xk_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
+                                       ctypes.POINTER(XkRequestStats)]),
+    "xk_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkServerStats)]),
+    "xk_server_destroy": (None, [ctypes.c_void_p]),
     "xk_kirchhoff_auto": (ctypes.c_int, [
         ctypes.POINTER(XkGpuRay), ctypes.c_size_t, ctypes.POINTER(XkGpuPixel), ctypes.c_size_t,
         _dp]),
