@@ -62,9 +62,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sweep", type=int, default=-1, help="-1 auto, 0 SFU reciprocal, 1 packed")
     ap.add_argument("--phase-budget", type=float, default=256.0)
-    ap.add_argument("--workload", choices=["single", "batch", "sweep"], default="single",
+    ap.add_argument("--workload", choices=["single", "batch", "sweep", "serve"], default="single",
                     help="single: the 2^20 x 512^2 solve (default); batch: 64 uneven solves; "
                          "sweep: the energy x distance precision sweep")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate [1/s]")
+    ap.add_argument("--duration", type=float, default=60.0, help="serve: arrival window [s]")
+    ap.add_argument("--drain", type=float, default=60.0,
+                    help="serve: seconds to wait for outstanding requests after the window")
     ap.add_argument("--sweep-sample", type=int, default=64,
                     help="screen points per cell checked against the CPU oracle")
     ap.add_argument("--batch-count", type=int, default=64)
@@ -337,6 +341,117 @@ def run_sweep(args):
     return 0
 
 
+def run_serve(args):
+    """Poisson request stream through the continuous-batching server.
+
+    Request sizes follow the serving configuration (rays log-uniform in
+    [1e4, 2e6], screen points log-uniform in [256, 1e6], E ~ U(1, 30) keV,
+    d ~ U(100, 20000) mm, 30 % reuse a resident ray set). Rays are slices of a
+    shared 2e6-ray Gaussian aperture with the request's energy, so requests
+    can be produced at the arrival rate; screens are square grids."""
+    import threading
+
+    import torch
+    import xrt_rs
+    from xrt_rs import synth
+    from xrt_rs.serve import Server
+
+    torch.cuda.set_device(0)
+    ctx = xrt_rs.GpuContext.new(0)
+    reqs = synth.config4_requests(seed=0, rate_hz=args.rate, duration_s=args.duration)
+    base = synth.gaussian_aperture(2_000_000, 0.1, 10_000.0, 30_000.0, seed=1)
+    srv = Server(ctx, hbm_budget_bytes=120e9)
+    sets = {}
+    lat, done_pairs, failures = [], [0.0], [0]
+    lock = threading.Lock()
+    pending = []
+
+    def rays_for(r):
+        n = r["n_rays"]
+        out = {k: v[:n] for k, v in base.items() if k != "energy"}
+        out["energy"] = np.full(n, r["energy_ev"])
+        return out
+
+    def screen_for(r):
+        side = max(16, int(round(np.sqrt(r["n_pix"]))))
+        return synth.grid_screen(side, side, 1.0, r["dist_mm"])
+
+    def waiter():
+        while True:
+            with lock:
+                item = pending.pop(0) if pending else None
+            if item is None:
+                if stop.is_set():
+                    return
+                time.sleep(0.001)
+                continue
+            t, pairs = item
+            try:
+                srv.wait(t, timeout_ms=max(1.0, 1e3 * (deadline - time.perf_counter())))
+                st = srv.last_stats
+                with lock:
+                    lat.append(st["total_ms"])
+                    done_pairs[0] += st["pairs"]
+            except xrt_rs.XkError:
+                with lock:
+                    failures[0] += 1
+
+    stop = threading.Event()
+    deadline = time.perf_counter() + args.duration + args.drain + 5
+    waiters = [threading.Thread(target=waiter, daemon=True) for _ in range(8)]
+    for w in waiters:
+        w.start()
+    t0 = time.perf_counter()
+    submitted = 0
+    for i, r in enumerate(reqs):
+        now = time.perf_counter() - t0
+        if r["t"] > now:
+            time.sleep(r["t"] - now)
+        screen = screen_for(r)
+        if r["reuse_of"] >= 0 and sets:
+            # A new screen on a ray set already resident on the device.
+            key = list(sets)[r["reuse_of"] % len(sets)]
+            handle, n = sets[key]
+            t = srv.submit(screen, rayset=handle)
+        else:
+            rays = rays_for(r)
+            n = r["n_rays"]
+            if i % 4 == 0:  # keep up to 32 ray sets resident for later screens
+                if len(sets) >= 32:
+                    old = next(iter(sets))
+                    srv.release_rays(sets.pop(old)[0])
+                sets[i] = (srv.upload_rays(rays), n)
+                t = srv.submit(screen, rayset=sets[i][0])
+            else:
+                t = srv.submit(screen, rays=rays)
+        with lock:
+            pending.append((t, float(n) * len(screen["x"])))
+        submitted += 1
+    window = time.perf_counter() - t0
+    stop.set()
+    for w in waiters:
+        w.join(timeout=args.drain + 30)
+    elapsed = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    ctx.close()
+    lat_a = np.array(lat) if lat else np.array([np.nan])
+    line = {
+        "workload": "serve", "metric": "served latency and throughput", "rate_hz": args.rate,
+        "window_s": window, "elapsed_s": elapsed, "submitted": submitted,
+        "completed": len(lat), "failed_or_unfinished": submitted - len(lat),
+        "p50_ms": float(np.percentile(lat_a, 50)), "p90_ms": float(np.percentile(lat_a, 90)),
+        "p99_ms": float(np.percentile(lat_a, 99)),
+        "gpair_s_served": done_pairs[0] / elapsed / 1e9,
+        "offered_gpair_s": sum(r["n_rays"] * max(16, int(round(np.sqrt(r["n_pix"])))) ** 2
+                               for r in reqs) / args.duration / 1e9,
+        "epochs": st["epochs"], "peak_bytes": st["peak_bytes"], "hbm_budget_bytes": 120e9,
+        "data": "synthetic: rays sliced from one 2e6-ray aperture, square-grid screens",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -345,6 +460,8 @@ def main():
         return run_batch(args)
     if args.workload == "sweep":
         return run_sweep(args)
+    if args.workload == "serve":
+        return run_serve(args)
 
     import torch
     import xrt_rs

@@ -297,7 +297,9 @@ int xk_server_wait(xk_server* server, uint64_t ticket, double timeout_ms,
 
 int xk_server_get_stats(xk_server* server, xk_server_stats* out);
 
-/* Stops admitting, finishes admitted requests, cancels pending ones. */
+/* Stops: waits for the epochs already launched, then cancels every request
+ * not yet completed (their waits return XK_ERR_SHUTDOWN) and frees the server.
+ * Tickets are invalid afterwards. */
 void xk_server_destroy(xk_server* server);
 
 /* ---- allocation-free FP64 solve ---------------------------------------------

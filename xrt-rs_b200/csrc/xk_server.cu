@@ -7,7 +7,7 @@
 // launch over items of every admitted request — a fair share of the epoch's
 // pair budget per request — so requests that arrive while others are on the
 // GPU join the next epoch and their work runs on the device together with
-// the older requests'. Two epochs are kept in flight. When a request's last
+// the older requests'. Up to three epochs are queued. When a request's last
 // items have been launched, its final reduction follows on the same stream;
 // a completion thread copies the field to the caller's buffers, frees the
 // request's memory and wakes waiters.
@@ -372,14 +372,25 @@ void worker_loop(xk_server* s) {
                 return false;
             };
             if (!idle()) s->cv_work.wait_for(lock, std::chrono::milliseconds(2), idle);
-            if (s->stopping && s->pending.empty() && s->active.empty()) break;
             if (s->stopping) {
-                // Cancel what has not started.
+                // Let the launched epochs finish (no kernel may touch memory
+                // that is about to be freed), then cancel everything else.
+                lock.unlock();
+                for (EpochSlot& e : s->slots) retire_slot(s, e);
+                lock.lock();
                 while (!s->pending.empty()) {
                     Req* q = s->pending.front();
                     s->pending.pop_front();
                     finish_request(s, q, XK_ERR_SHUTDOWN);
                 }
+                for (Req* q : s->active) {
+                    q->status = XK_ERR_SHUTDOWN;
+                    q->state = ReqState::Computed;
+                    s->computed.push_back(q);
+                }
+                s->active.clear();
+                s->cv_work.notify_all();
+                break;
             }
             // Admission: FIFO while the budget and the slot count allow.
             while (!s->pending.empty() && (int)s->active.size() < s->opts.max_active) {
@@ -429,6 +440,11 @@ void worker_loop(xk_server* s) {
         }
         if (runnable.empty()) continue;
         xk::Status st = run_epoch(s, runnable);
+        if (!st.ok()) {
+            // Requests leave with an error: let launched epochs finish first.
+            cudaGetLastError();
+            for (EpochSlot& e : s->slots) retire_slot(s, e);
+        }
         std::lock_guard<std::mutex> lock(s->mu);
         if (!st.ok()) s->last_error = st.msg;
         for (Req* q : runnable) {
