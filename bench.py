@@ -286,6 +286,8 @@ def run_sweep(args):
 
     torch.cuda.set_device(0)
     ctx = xrt_rs.GpuContext.new(0)
+    ctx.set_option("sweep", args.sweep)
+    ctx.set_option("phase_budget", args.phase_budget)
     cells = []
     for e in synth.CONFIG2_ENERGIES:
         for d in synth.CONFIG2_DISTANCES:
@@ -372,9 +374,15 @@ def run_serve(args):
         out["energy"] = np.full(n, r["energy_ev"])
         return out
 
+    grids = {}
+
     def screen_for(r):
         side = max(16, int(round(np.sqrt(r["n_pix"]))))
-        return synth.grid_screen(side, side, 1.0, r["dist_mm"])
+        if side not in grids:
+            g = synth.grid_screen(side, side, 1.0, 0.0)
+            grids[side] = (g["x"], g["y"])
+        x, y = grids[side]
+        return {"x": x, "y": y, "z": np.full(len(x), r["dist_mm"])}
 
     def waiter():
         while True:
@@ -529,10 +537,8 @@ def main():
     clk = clocks.stop()
     ms = float(np.mean(step_ms))
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        from xrt_rs import parallel
+        ms = parallel.max_over_ranks(ms)
     value = pairs * world / (ms / 1e3) / 1e9
     out32 = [t.cpu().numpy() for t in d_out]
 
@@ -553,10 +559,8 @@ def main():
             times.append(time.perf_counter() - t0)
         e2e_ms = 1e3 * float(np.mean(times))
         if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+            from xrt_rs import parallel
+            e2e_ms = parallel.max_over_ranks(e2e_ms)
         e2e = {"value": pairs * world / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
                "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(st["h2d_bytes"]),
                "d2h_bytes_per_step": int(st["d2h_bytes"])}

@@ -147,6 +147,24 @@ const char* xk_route_reason(int reason);
  *   "items_per_warp" target work items per resident warp (automatic groups) */
 int xk_set_option(xk_ctx* ctx, const char* name, double value);
 
+typedef struct xk_tune_result {
+    double default_ms;       /* device time of the solve with the options in force */
+    double best_ms;          /* device time with the best options found */
+    double phase_budget;     /* best "phase_budget" (ray-chunk size) */
+    long long items_per_warp;/* best "items_per_warp" (ray groups per tile) */
+    int sweep;               /* best "sweep" */
+    int trials;
+} xk_tune_result;
+
+/* Autotuner (no counterpart in the reference): times the XK_PATH_F32PR solve
+ * of this device-resident problem under candidate settings of the knobs above
+ * (residual-phase budget, i.e. ray-chunk size, up to 512 rad; work items per
+ * warp; sweep variant) until `budget_ms` of device time is spent, writes the
+ * field into `out`, and with `apply` keeps the fastest settings on `ctx`. */
+int xk_autotune(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_pixels* pixels,
+                size_t n_pix, xk_field* out, double budget_ms, int apply,
+                xk_tune_result* result);
+
 /* ---- single solves --------------------------------------------------------- */
 
 /* waves::diffraction::diffraction_integral (src/waves/diffraction.rs:56-64)
@@ -249,6 +267,7 @@ typedef struct xk_server_opts {
     int max_active;                   /* admitted requests at once; 0 = 64 */
     double item_pairs;                /* target pairs per work item; 0 = 4e6 */
     int inject_alloc_failure_every;   /* testing: fail every k-th request allocation; 0 = off */
+    int reserve_sms;                  /* SMs epochs leave free for planning kernels; 0 = 8 */
 } xk_server_opts;
 
 typedef struct xk_request {

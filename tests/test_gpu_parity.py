@@ -244,3 +244,20 @@ def test_f32pr_extreme_cells_vs_extended_oracle(ctx, oracle, energy, dist):
     print(f"E={energy} d={dist}: f32pr vs exact {err:.2e}, fp64 formula vs exact {f64_err:.2e}, "
           f"chunks={st['n_chunks']} path={st['path']}")
     assert err < PR_TOL
+
+
+def test_autotune_keeps_results_and_restores_options(ctx, oracle):
+    torch = pytest.importorskip("torch")
+    rays, pix = synth.config0(seed=6)
+    rl, pl = cases.as_lists(rays, pix)
+    d_r = [torch.from_numpy(a).cuda() for a in rl]
+    d_p = [torch.from_numpy(a).cuda() for a in pl]
+    d_o = [torch.zeros(len(pl[0]), dtype=torch.float64, device="cuda") for _ in range(4)]
+    res = xrt_rs.autotune(d_r, d_p, d_o, ctx=ctx, budget_ms=50.0, apply=False)
+    assert res["trials"] >= 1 and res["best_ms"] <= res["default_ms"] + 1e-9
+    assert res["phase_budget"] <= 512.0
+    out = [t.cpu().numpy() for t in d_o]
+    assert cases.rel_l2(out, oracle.kahan_ld(rl, pl)) < PR_TOL
+    # apply=False left the context's defaults in force
+    _, st = run(ctx, rays, pix, "f32pr")
+    assert st["phase_bound_rad"] <= 256.0 + 1e-9

@@ -259,6 +259,67 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
     return XK_OK;
 }
 
+int xk_autotune(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_pixels* pixels,
+                size_t n_pix, xk_field* out, double budget_ms, int apply,
+                xk_tune_result* result) {
+    if (!ctx || !result) return XK_ERR_INVALID;
+    if (!rays_ok(rays) || !pix_ok(pixels) || !field_ok(out) || n_rays == 0 || n_pix == 0)
+        return fail(ctx, XK_ERR_INVALID, "autotune needs a non-empty device-resident problem");
+    std::memset(result, 0, sizeof(*result));
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    const xk::RaysDev rd = to_dev(rays);
+    const xk::PixDev pd{pixels->x, pixels->y, pixels->z};
+    const xk::FieldDev fd{out->es_re, out->es_im, out->ep_re, out->ep_im};
+    const xk::PrOptions base = ctx->pr_opts;
+    // Candidates: the defaults first, then larger and smaller residual-phase
+    // budgets (ray chunks grow with the budget; the FP32 error bound grows
+    // with it too, so the search stops at 512 rad), more or fewer items per
+    // warp, and the SFU sweep.
+    struct Cand {
+        double budget;
+        long long ipw;
+        int sweep;
+    };
+    const Cand cands[] = {{base.phase_budget, base.items_per_warp, base.sweep},
+                          {512.0, 16, -1}, {128.0, 16, -1}, {256.0, 32, -1}, {256.0, 8, -1},
+                          {512.0, 32, -1}, {512.0, 8, -1}, {256.0, 16, 0}, {512.0, 16, 0}};
+    double spent = 0.0, best = 1e300;
+    xk::PrOptions best_opt = base;
+    int trials = 0;
+    for (const Cand& c : cands) {
+        if (trials > 0 && spent >= budget_ms) break;
+        ctx->pr_opts = base;
+        ctx->pr_opts.phase_budget = std::min(c.budget, 512.0);
+        ctx->pr_opts.items_per_warp = c.ipw;
+        ctx->pr_opts.sweep = c.sweep;
+        xk_stats st;
+        std::memset(&st, 0, sizeof(st));
+        int used = XK_PATH_F32PR;
+        xk::Status s = run_solve(ctx, rd, n_rays, pd, n_pix, fd, XK_PATH_F32PR, ctx->stream, &st, &used);
+        if (s.ok()) s = finish_stats(ctx, &st, used, n_rays, n_pix);
+        if (!s.ok()) {
+            ctx->pr_opts = base;
+            return fail(ctx, s);
+        }
+        ++trials;
+        spent += st.gpu_ms;
+        if (trials == 1) result->default_ms = st.gpu_ms;
+        if (used != XK_PATH_F32PR) break;  // routed to FP64: nothing to tune
+        if (st.gpu_ms < best) {
+            best = st.gpu_ms;
+            best_opt = ctx->pr_opts;
+        }
+    }
+    ctx->pr_opts = apply ? best_opt : base;
+    result->best_ms = best < 1e299 ? best : result->default_ms;
+    result->phase_budget = best_opt.phase_budget;
+    result->items_per_warp = best_opt.items_per_warp;
+    result->sweep = best_opt.sweep;
+    result->trials = trials;
+    return XK_OK;
+}
+
 int xk_diffraction_integral(xk_ctx* ctx, const xk_rays* rays, size_t n_rays,
                             const xk_pixels* pixels, size_t n_pix, xk_field* out, int path,
                             xk_stats* stats) {

@@ -55,6 +55,8 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kSumFields = 26;
 constexpr uint32_t kMaxWaitIters = 1u << 24;
+// Stages of FP32 partial sums per fold into the two-float accumulators.
+constexpr int kFoldStages = 1;
 // |e| bound under which the packed sweep's series reciprocal is used.
 constexpr double kSeriesRcpBound = 2e-3;
 
@@ -561,15 +563,62 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
     }
 }
 
+// Adds the lane's FP32 partials into its two-float accumulators and clears
+// them (every kFoldStages stages and at chunk and item ends).
+template <bool UNIFORM>
+__device__ __forceinline__ void fold_acc(ScalarState<UNIFORM>& ls, WarpShared& ws, int lane) {
+#pragma unroll
+    for (int i = 0; i < kPrPpl; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float hi = ws.hi[i * 4 + c][lane], lo = ws.lo[i * 4 + c][lane];
+            two_sum_acc(hi, lo, ls.acc[i][c]);
+            ws.hi[i * 4 + c][lane] = hi;
+            ws.lo[i * 4 + c][lane] = lo;
+            ls.acc[i][c] = 0.f;
+        }
+}
+
+template <bool UNIFORM>
+__device__ __forceinline__ void fold_acc(PackedState<UNIFORM>& ls, WarpShared& ws, int lane) {
+#pragma unroll
+    for (int i = 0; i < kPrPpl / 2; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float2 v = ls.acc[i][c];
+            float hi0 = ws.hi[(2 * i) * 4 + c][lane], lo0 = ws.lo[(2 * i) * 4 + c][lane];
+            float hi1 = ws.hi[(2 * i + 1) * 4 + c][lane], lo1 = ws.lo[(2 * i + 1) * 4 + c][lane];
+            two_sum_acc(hi0, lo0, v.x);
+            two_sum_acc(hi1, lo1, v.y);
+            ws.hi[(2 * i) * 4 + c][lane] = hi0;
+            ws.lo[(2 * i) * 4 + c][lane] = lo0;
+            ws.hi[(2 * i + 1) * 4 + c][lane] = hi1;
+            ws.lo[(2 * i + 1) * 4 + c][lane] = lo1;
+            ls.acc[i][c] = f2(0.f);
+        }
+}
+
+template <bool UNIFORM>
+__device__ __forceinline__ void clear_acc(ScalarState<UNIFORM>& ls) {
+#pragma unroll
+    for (int i = 0; i < kPrPpl; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ls.acc[i][c] = 0.f;
+}
+
+template <bool UNIFORM>
+__device__ __forceinline__ void clear_acc(PackedState<UNIFORM>& ls) {
+#pragma unroll
+    for (int i = 0; i < kPrPpl / 2; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ls.acc[i][c] = f2(0.f);
+}
+
 // SFU sweep: one point per FP32 instruction, rcp.approx for the reciprocal.
 template <bool UNIFORM>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
                                             ScalarState<UNIFORM>& ls, WarpShared& ws) {
     const float4* rec = reinterpret_cast<const float4*>(buf);
-#pragma unroll
-    for (int i = 0; i < kPrPpl; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) ls.acc[i][c] = 0.f;
 #pragma unroll 1
     for (int j = 0; j < len; ++j) {
         const float4 a = rec[4 * j + 0];
@@ -601,15 +650,6 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             ls.acc[i][3] = fmaf(e.z, as, fmaf(e.w, ac, ls.acc[i][3]));
         }
     }
-#pragma unroll
-    for (int i = 0; i < kPrPpl; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            float hi = ws.hi[i * 4 + c][lane], lo = ws.lo[i * 4 + c][lane];
-            two_sum_acc(hi, lo, ls.acc[i][c]);
-            ws.hi[i * 4 + c][lane] = hi;
-            ws.lo[i * 4 + c][lane] = lo;
-        }
 }
 
 // Packed sweep: two points per f32x2 instruction, series reciprocal.
@@ -618,10 +658,6 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
                                             PackedState<UNIFORM>& ls, WarpShared& ws) {
     constexpr int H = kPrPpl / 2;
     const float4* rec = reinterpret_cast<const float4*>(buf);
-#pragma unroll
-    for (int i = 0; i < H; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) ls.acc[i][c] = f2(0.f);
 #pragma unroll 1
     for (int j = 0; j < len; ++j) {
         const float4 a = rec[4 * j + 0];
@@ -662,20 +698,6 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             ls.acc[i][3] = __ffma2_rn(ez, as, __ffma2_rn(ew, ac, ls.acc[i][3]));
         }
     }
-#pragma unroll
-    for (int i = 0; i < H; ++i)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const float2 v = ls.acc[i][c];
-            float hi0 = ws.hi[(2 * i) * 4 + c][lane], lo0 = ws.lo[(2 * i) * 4 + c][lane];
-            float hi1 = ws.hi[(2 * i + 1) * 4 + c][lane], lo1 = ws.lo[(2 * i + 1) * 4 + c][lane];
-            two_sum_acc(hi0, lo0, v.x);
-            two_sum_acc(hi1, lo1, v.y);
-            ws.hi[(2 * i) * 4 + c][lane] = hi0;
-            ws.lo[(2 * i) * 4 + c][lane] = lo0;
-            ws.hi[(2 * i + 1) * 4 + c][lane] = hi1;
-            ws.lo[(2 * i + 1) * 4 + c][lane] = lo1;
-        }
 }
 
 struct WarpPipe {
@@ -729,6 +751,8 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
 
     using State = typename std::conditional<FAST, PackedState<UNIFORM>, ScalarState<UNIFORM>>::type;
     State st;
+    clear_acc(st);
+    int since_fold = 0;
     int cur_chunk = -1;
     int pos = r0;
     int c = chunk_of(cb, n_chunks, pos);
@@ -779,6 +803,11 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
         prep_stage(wp.buf[b], len, lane, sv, ws);
         __syncwarp();
         sweep_stage<UNIFORM>(wp.buf[b], len, lane, st, ws);
+        // FP32 partials run over at most kFoldStages stages of one chunk.
+        if (++since_fold == kFoldStages || nlen == 0 || nc != c) {
+            fold_acc(st, ws, lane);
+            since_fold = 0;
+        }
         // Order this stage's generic-proxy accesses before the next bulk
         // copy into the same buffer.
         fence_proxy_async();
@@ -1047,7 +1076,8 @@ size_t pr_plan_bytes(size_t n, size_t m, int num_sms, const PrOptions& opt) {
 }
 
 Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t stream, int num_sms,
-               const PrOptions& opt, std::vector<PrPlan>& plans, int* kernels) {
+               const PrOptions& opt, std::vector<PrPlan>& plans, int* kernels,
+               DevBuf* const* arenas) {
     plans.assign(count, PrPlan());
     int nk = 0;
     const int sum_blocks = sum_blocks_for(num_sms);
@@ -1078,13 +1108,14 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
                                                     (int*)nullptr, m));
         XK_CUDA_TRY(cub::DeviceScan::InclusiveSum(nullptr, c3, (int*)nullptr, (int*)nullptr, n));
         cub_need = std::max(cub_need, std::max(c1, std::max(c2, c3)));
-        Arena a{nullptr, need};
+        Arena a{nullptr, arenas ? 0 : need};
         SolveBufs b;
         carve(a, b, n, m, n_tiles[s], g, sum_blocks);
-        need = a.off;
+        if (arenas) XK_TRY(arenas[s]->ensure(a.off + 256));
+        else need = a.off;
     }
     XK_TRY(ws.cub_tmp.ensure(cub_need + 256));
-    XK_TRY(ws.arena.ensure(need + 256));
+    if (!arenas) XK_TRY(ws.arena.ensure(need + 256));
     const HostLayout HL = host_layout(count, sum_blocks);
     XK_TRY(ws.ensure_host(HL.total));
     char* hbase = static_cast<char*>(ws.host);
@@ -1097,7 +1128,7 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         size_t off = 0;
         for (int s = 0; s < count; ++s) {
             if (plans[s].routed) continue;
-            Arena a{ws.arena.as<char>(), off};
+            Arena a{arenas ? arenas[s]->as<char>() : ws.arena.as<char>(), arenas ? 0 : off};
             carve(a, bufs[s], (int)in[s].n, (int)in[s].m, n_tiles[s], groups[s], sum_blocks);
             off = a.off;
         }
@@ -1384,6 +1415,10 @@ Status pr_finalize(const PrPlan& P, cudaStream_t stream) {
                                                              slots, P.out);
     XK_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
+}
+
+Status pr_reserve_plan_host(PrWorkspace& ws, int count, int num_sms) {
+    return ws.ensure_host(host_layout(count, sum_blocks_for(num_sms)).total);
 }
 
 Status pr_reserve_exec(PrWorkspace& ws, int count, int num_sms) {

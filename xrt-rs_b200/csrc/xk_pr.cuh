@@ -110,12 +110,18 @@ struct PrWorkspace {
 size_t pr_plan_bytes(size_t n, size_t m, int num_sms, const PrOptions& opt);
 
 // Plans `count` solves in one pass (three host synchronisations for the
-// whole batch). Plans reference memory in ws.arena until the next call.
+// whole batch). Plans reference memory in ws.arena until the next call, or,
+// with `arenas`, solve s's memory in *arenas[s] (grown as needed), so that
+// solves planned together can be released one by one.
 Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t stream, int num_sms,
-               const PrOptions& opt, std::vector<PrPlan>& plans, int* kernels);
+               const PrOptions& opt, std::vector<PrPlan>& plans, int* kernels,
+               DevBuf* const* arenas = nullptr);
 
 // Allocates everything pr_execute_enqueue needs for `count` solves, so that a
 // following enqueue allocates nothing (required while capturing a graph).
+// Pinned readback area for planning up to `count` solves at once (so that a
+// long-lived planner never reallocates it).
+Status pr_reserve_plan_host(PrWorkspace& ws, int count, int num_sms);
 Status pr_reserve_exec(PrWorkspace& ws, int count, int num_sms);
 
 // Enqueues the sweep of every non-routed plan: per kernel variant one

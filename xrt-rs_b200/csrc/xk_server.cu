@@ -1,16 +1,19 @@
 // Continuous-batching Kirchhoff server.
 //
-// Requests (solves of any size) arrive from any thread. A worker thread
-// admits them while the admitted set fits an HBM budget, copies their inputs
-// (or uses a resident ray set), plans them on a high-priority planning stream
-// and slices their work items into epochs: each epoch is one persistent
-// launch over items of every admitted request — a fair share of the epoch's
-// pair budget per request — so requests that arrive while others are on the
-// GPU join the next epoch and their work runs on the device together with
-// the older requests'. Up to three epochs are queued. When a request's last
-// items have been launched, its final reduction follows on the same stream;
-// a completion thread copies the field to the caller's buffers, frees the
-// request's memory and wakes waiters.
+// Requests (solves of any size) arrive from any thread. Three threads serve
+// them:
+//   * the scheduler admits requests while the admitted set fits an HBM
+//     budget and the slot count, and launches epochs: each epoch is one
+//     persistent launch over work items of every planned request — a fair
+//     share of the epoch's pair budget each — so requests that arrive while
+//     others are on the GPU join the next epoch and run on the device
+//     together with the older ones. Up to three epochs are queued, and epochs
+//     leave a few SMs free so that planning kernels never wait behind them;
+//   * the planner copies the inputs of newly admitted requests (or uses a
+//     resident ray set) and plans all of them in one batched pass on a
+//     high-priority stream (three host synchronisations per batch);
+//   * the finisher waits for a request's final reduction, copies its field to
+//     the caller's buffers, frees its memory and wakes waiters.
 //
 // Results are independent of the mix: a request's items accumulate into its
 // own slots in a fixed order (sub-ranges of a ray group in sub order, groups
@@ -22,6 +25,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -62,9 +66,9 @@ struct Req {
     int path = XK_PATH_F32PR;
     bool routed = false;
     // device state
-    xk::DevBuf mem;  // inputs (unless a ray set), screen points, output field
-    xk::PrWorkspace ws;
-    std::vector<xk::PrPlan> plans;
+    xk::DevBuf mem;    // inputs (unless a ray set), screen points, output field
+    xk::DevBuf arena;  // the plan's memory
+    xk::PrPlan plan;
     xk::PrSolveIn in{};
     long long n_items = 0, next_item = 0, slice_cap = 0;
     double pairs_per_item = 0.0;
@@ -72,12 +76,11 @@ struct Req {
     int epochs = 0;
     Clock::time_point t_submit, t_admit, t_planned, t_done;
     RaySet* rayset = nullptr;
-    void* pinned = nullptr;  // borrowed planning readback area
 };
 
 constexpr int kEpochRing = 3;
-constexpr size_t kPinnedBlock = 256 << 10;  // planning readback area of one solve
 constexpr int kVariants = 4;
+constexpr int kPlanBatch = 32;  // requests planned together at most
 
 struct EpochSlot {
     xk::DevBuf table;     // PrSolve entries
@@ -97,23 +100,23 @@ struct xk_server {
     xk::PrOptions pr_opts;
     int num_sms = 0;
     cudaStream_t plan_stream = nullptr, exec_stream = nullptr, io_stream = nullptr,
-                 f64_stream = nullptr;
+                 f64_stream = nullptr, out_stream = nullptr;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
-    std::deque<Req*> pending;
-    std::vector<Req*> active;  // admitted, not yet computed
-    std::deque<Req*> computed;  // waiting for the completion thread
+    std::condition_variable cv_work, cv_plan, cv_done;
+    std::deque<Req*> pending;    // submitted, not admitted
+    std::deque<Req*> to_plan;    // admitted, waiting for the planner
+    std::vector<Req*> active;    // admitted, not yet computed
+    std::deque<Req*> computed;   // waiting for the finisher
     std::unordered_map<uint64_t, Req*> reqs;
     std::unordered_map<uint64_t, RaySet*> raysets;
     uint64_t next_ticket = 1, next_rayset = 1;
     double used_bytes = 0.0, peak_bytes = 0.0, ray_bytes = 0.0;
-    bool stopping = false;
-    std::thread worker, finisher;
+    bool stopping = false, planner_done = false, worker_done = false;
+    std::thread worker, planner, finisher;
     EpochSlot slots[kEpochRing];
     int next_slot = 0;
+    xk::PrWorkspace plan_ws;  // planner's CUB scratch and pinned readback area
     xk::F64Workspace f64ws;
-    std::vector<void*> pinned_free;  // planning readback areas, one per admitted request
-    std::vector<void*> pinned_all;
     long long alloc_count = 0;
     // statistics
     long long submitted = 0, completed = 0, failed = 0;
@@ -124,10 +127,14 @@ struct xk_server {
 
 namespace {
 
-// Device allocation that counts against the budget's fault injector.
+// Device allocation that counts against the fault injector.
 xk::Status checked_ensure(xk_server* s, xk::DevBuf& b, size_t bytes) {
     if (s->opts.inject_alloc_failure_every > 0) {
-        long long c = ++s->alloc_count;
+        long long c;
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            c = ++s->alloc_count;
+        }
         if (c % s->opts.inject_alloc_failure_every == 0)
             return xk::Status::Err(XK_ERR_OOM, "injected allocation failure");
     }
@@ -159,8 +166,29 @@ void finish_request(xk_server* s, Req* q, int status) {
     s->cv_work.notify_all();
 }
 
-// Copies inputs, plans (FP32-PR) or enqueues the FP64 path. Runs on the worker.
-xk::Status setup_request(xk_server* s, Req* q) {
+// Caller holds s->mu: the request leaves `active` for the finisher.
+void to_computed(xk_server* s, Req* q, int status) {
+    if (status != XK_OK) q->status = status;
+    q->state = ReqState::Computed;
+    auto it = std::find(s->active.begin(), s->active.end(), q);
+    if (it != s->active.end()) s->active.erase(it);
+    s->computed.push_back(q);
+    s->cv_work.notify_all();
+}
+
+xk::Status record_and_wait(cudaStream_t from, cudaStream_t to) {
+    cudaEvent_t ev;
+    XK_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e1 = cudaEventRecord(ev, from);
+    cudaError_t e2 = cudaStreamWaitEvent(to, ev, 0);
+    cudaEventDestroy(ev);
+    XK_CUDA_TRY(e1);
+    XK_CUDA_TRY(e2);
+    return xk::Status::Ok();
+}
+
+// Device buffers and host-to-device copies of one request (io stream).
+xk::Status copy_inputs(xk_server* s, Req* q) {
     const xk_request& r = q->r;
     const size_t n = q->rayset ? q->rayset->n : r.n_rays;
     const size_t m = r.n_pix;
@@ -195,63 +223,94 @@ xk::Status setup_request(xk_server* s, Req* q) {
     }
     q->in.n = n;
     q->in.m = m;
-    // Planning reads the inputs: order the planning stream after the copies.
-    cudaEvent_t copied;
-    XK_CUDA_TRY(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
-    XK_CUDA_TRY(cudaEventRecord(copied, s->io_stream));
-    XK_CUDA_TRY(cudaStreamWaitEvent(s->plan_stream, copied, 0));
-    cudaEventDestroy(copied);
-
     XK_CUDA_TRY(cudaEventCreateWithFlags(&q->done_ev, cudaEventDisableTiming));
-    if (q->path == XK_PATH_F32PR) {
-        q->ws.set_async(s->plan_stream);
-        {
-            std::lock_guard<std::mutex> lock(s->mu);
-            if (s->pinned_free.empty()) return xk::Status::Err(XK_ERR_OOM, "no planning area free");
-            q->pinned = s->pinned_free.back();
-            s->pinned_free.pop_back();
-        }
-        q->ws.host = q->pinned;
-        q->ws.host_bytes = kPinnedBlock;
-        q->ws.host_borrowed = true;
-        int nk = 0;
-        XK_TRY(xk::pr_plan(&q->in, 1, q->ws, s->plan_stream, s->num_sms, s->pr_opts, q->plans, &nk));
-        s->kernels += nk;
-        xk::PrPlan& P = q->plans[0];
-        q->routed = P.routed;
-        if (!P.routed) {
-            // Slice every ray group into sub-ranges of about item_pairs pairs.
-            const double rays_per_group = (double)n / P.groups;
-            int subs = (int)std::ceil(rays_per_group * xk::kPrTile / s->opts.item_pairs);
-            subs = std::max(1, std::min(subs, std::max(1, (int)(rays_per_group / xk::kPrStage))));
-            P.dev.subs = subs;
-            P.dev.n_items = (long long)P.n_tiles * P.groups * subs;
-            q->n_items = P.dev.n_items;
-            q->slice_cap = (long long)P.n_tiles * P.groups;
-            q->pairs_per_item = rays_per_group / subs * xk::kPrTile;
-            XK_TRY(xk::pr_zero_partials(P, s->plan_stream));
-            // The execution stream must see the plan and the cleared slots.
-            cudaEvent_t planned;
-            XK_CUDA_TRY(cudaEventCreateWithFlags(&planned, cudaEventDisableTiming));
-            XK_CUDA_TRY(cudaEventRecord(planned, s->plan_stream));
-            XK_CUDA_TRY(cudaStreamWaitEvent(s->exec_stream, planned, 0));
-            cudaEventDestroy(planned);
-            return xk::Status::Ok();
-        }
-    }
-    // FP64 path (requested, or routed by the planner): one launch on its own stream.
+    return xk::Status::Ok();
+}
+
+// The FP64 path for one request (requested, or routed by the planner).
+xk::Status launch_f64(xk_server* s, Req* q) {
     q->routed = true;
-    cudaEvent_t ready;
-    XK_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-    XK_CUDA_TRY(cudaEventRecord(ready, s->plan_stream));
-    XK_CUDA_TRY(cudaStreamWaitEvent(s->f64_stream, ready, 0));
-    cudaEventDestroy(ready);
+    XK_TRY(record_and_wait(s->plan_stream, s->f64_stream));
     xk::LaunchReport rep;
-    XK_TRY(xk::f64_enqueue(q->in.rays, n, q->in.pix, m, q->in.out, s->f64ws, s->f64_stream,
-                           s->num_sms, &rep));
+    XK_TRY(xk::f64_enqueue(q->in.rays, q->in.n, q->in.pix, q->in.m, q->in.out, s->f64ws,
+                           s->f64_stream, s->num_sms, &rep));
     s->kernels += rep.kernels;
     XK_CUDA_TRY(cudaEventRecord(q->done_ev, s->f64_stream));
     return xk::Status::Ok();
+}
+
+// Copies and plans a batch of admitted requests; runs on the planner thread.
+void plan_batch(xk_server* s, std::vector<Req*>& batch) {
+    std::vector<Req*> ok, pr;
+    for (Req* q : batch) {
+        xk::Status st = copy_inputs(s, q);
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (!st.ok()) {
+            s->last_error = st.msg;
+            q->t_planned = Clock::now();
+            to_computed(s, q, st.code);
+            continue;
+        }
+        ok.push_back(q);
+    }
+    if (ok.empty()) return;
+    xk::Status st = record_and_wait(s->io_stream, s->plan_stream);
+    for (Req* q : ok)
+        if (q->path == XK_PATH_F32PR) pr.push_back(q);
+    std::vector<xk::PrPlan> plans;
+    if (st.ok() && !pr.empty()) {
+        std::vector<xk::PrSolveIn> in;
+        std::vector<xk::DevBuf*> arenas;
+        for (Req* q : pr) {
+            q->arena.async_stream = s->plan_stream;
+            in.push_back(q->in);
+            arenas.push_back(&q->arena);
+        }
+        int nk = 0;
+        st = xk::pr_plan(in.data(), (int)in.size(), s->plan_ws, s->plan_stream, s->num_sms,
+                         s->pr_opts, plans, &nk, arenas.data());
+        s->kernels += nk;
+    }
+    for (size_t i = 0; st.ok() && i < pr.size(); ++i) {
+        Req* q = pr[i];
+        q->plan = plans[i];
+        xk::PrPlan& P = q->plan;
+        if (P.routed) continue;
+        // Slice every ray group into sub-ranges of about item_pairs pairs.
+        const double rays_per_group = (double)q->in.n / P.groups;
+        int subs = (int)std::ceil(rays_per_group * xk::kPrTile / s->opts.item_pairs);
+        subs = std::max(1, std::min(subs, std::max(1, (int)(rays_per_group / xk::kPrStage))));
+        P.dev.subs = subs;
+        P.dev.n_items = (long long)P.n_tiles * P.groups * subs;
+        q->n_items = P.dev.n_items;
+        q->slice_cap = (long long)P.n_tiles * P.groups;
+        q->pairs_per_item = rays_per_group / subs * xk::kPrTile;
+        st = xk::pr_zero_partials(P, s->plan_stream);
+    }
+    // The execution stream must see the plans and the cleared slots before
+    // the first epoch that includes these requests.
+    if (st.ok()) st = record_and_wait(s->plan_stream, s->exec_stream);
+    std::vector<Req*> f64;
+    for (Req* q : ok)
+        if (q->path == XK_PATH_F64 || q->plan.routed) f64.push_back(q);
+    for (Req* q : f64) {
+        if (!st.ok()) break;
+        st = launch_f64(s, q);
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (Req* q : ok) {
+        q->t_planned = Clock::now();
+        if (!st.ok()) {
+            s->last_error = st.msg;
+            cudaGetLastError();
+            to_computed(s, q, st.code);
+        } else if (q->routed) {
+            to_computed(s, q, XK_OK);
+        } else {
+            q->state = ReqState::Running;
+        }
+    }
+    s->cv_work.notify_all();
 }
 
 // Waits for an epoch slot's launch, checks its error word, frees the slot.
@@ -268,14 +327,13 @@ void retire_slot(xk_server* s, EpochSlot& e) {
     e.reqs.clear();
 }
 
-// Builds and launches one epoch over the admitted FP32-PR requests.
+// Builds and launches one epoch over the planned FP32-PR requests.
 xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
     EpochSlot& e = s->slots[s->next_slot];
     s->next_slot = (s->next_slot + 1) % kEpochRing;
     retire_slot(s, e);
 
-    const double budget = s->opts.epoch_pairs;
-    const double share = budget / std::max<size_t>(1, runnable.size());
+    const double share = s->opts.epoch_pairs / std::max<size_t>(1, runnable.size());
     struct Take {
         Req* q;
         long long first, count;
@@ -298,7 +356,7 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
         const bool uniform = (v & 1) != 0, fast = (v & 2) != 0;
         first[v] = tab;
         for (const Take& t : takes) {
-            xk::PrPlan& P = t.q->plans[0];
+            const xk::PrPlan& P = t.q->plan;
             if (P.uniform_normal != uniform || P.fast != fast) continue;
             xk::PrSolve d = P.dev;
             d.item_begin = counts[v];
@@ -313,10 +371,11 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
     XK_CUDA_TRY(cudaMemsetAsync(e.ctrl.ptr, 0, 256, s->exec_stream));
     unsigned long long* counters = e.ctrl.as<unsigned long long>();
     int* d_err = reinterpret_cast<int*>(e.ctrl.as<char>() + 128);
+    const int sms = std::max(1, s->num_sms - std::max(0, s->opts.reserve_sms));
     for (int v = 0; v < kVariants; ++v) {
         if (!nsol[v]) continue;
         XK_TRY(xk::pr_launch(e.table.as<xk::PrSolve>() + first[v], nsol[v], counts[v], (v & 1) != 0,
-                             (v & 2) != 0, counters + v, d_err, s->exec_stream, s->num_sms, 0));
+                             (v & 2) != 0, counters + v, d_err, s->exec_stream, sms, 0));
         s->kernels++;
     }
     XK_CUDA_TRY(cudaMemcpyAsync(e.h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s->exec_stream));
@@ -325,7 +384,7 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
         t.q->epochs++;
         e.reqs.push_back(t.q);
         if (t.q->next_item >= t.q->n_items) {
-            XK_TRY(xk::pr_finalize(t.q->plans[0], s->exec_stream));
+            XK_TRY(xk::pr_finalize(t.q->plan, s->exec_stream));
             s->kernels++;
             XK_CUDA_TRY(cudaEventRecord(t.q->done_ev, s->exec_stream));
         }
@@ -337,13 +396,11 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
 }
 
 void release_request_memory(xk_server* s, Req* q) {
-    q->ws.release();
+    q->arena.release();
     q->mem.release();
     if (q->done_ev) cudaEventDestroy(q->done_ev);
     q->done_ev = nullptr;
     std::lock_guard<std::mutex> lock(s->mu);
-    if (q->pinned) s->pinned_free.push_back(q->pinned);
-    q->pinned = nullptr;
     s->used_bytes -= q->bytes;
     if (q->rayset) {
         q->rayset->users--;
@@ -357,24 +414,52 @@ void release_request_memory(xk_server* s, Req* q) {
     }
 }
 
-void worker_loop(xk_server* s) {
+void planner_loop(xk_server* s) {
     cudaSetDevice(s->ctx->device);
-    // Plans of requests admitted in this turn, ordered by admission.
     while (true) {
-        std::vector<Req*> admitted;
+        std::vector<Req*> batch;
         {
             std::unique_lock<std::mutex> lock(s->mu);
-            auto idle = [&] {
+            s->cv_plan.wait_for(lock, std::chrono::milliseconds(5),
+                                [&] { return !s->to_plan.empty() || s->stopping; });
+            if (s->stopping) break;
+            while (!s->to_plan.empty() && (int)batch.size() < kPlanBatch) {
+                batch.push_back(s->to_plan.front());
+                s->to_plan.pop_front();
+            }
+        }
+        if (!batch.empty()) plan_batch(s, batch);
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->planner_done = true;
+    s->cv_work.notify_all();
+}
+
+void worker_loop(xk_server* s) {
+    cudaSetDevice(s->ctx->device);
+    while (true) {
+        std::vector<Req*> runnable;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            auto can_admit = [&] {
+                if (s->pending.empty() || (int)s->active.size() >= s->opts.max_active) return false;
+                const double b = s->pending.front()->bytes;
+                return s->active.empty() || b > s->opts.hbm_budget_bytes ||
+                       s->used_bytes + b <= s->opts.hbm_budget_bytes;
+            };
+            auto has_work = [&] {
                 if (s->stopping) return true;
-                if (!s->pending.empty() && (int)s->active.size() < s->opts.max_active) return true;
+                if (can_admit()) return true;
                 for (Req* q : s->active)
                     if (q->state == ReqState::Running && q->next_item < q->n_items) return true;
                 return false;
             };
-            if (!idle()) s->cv_work.wait_for(lock, std::chrono::milliseconds(2), idle);
+            if (!has_work()) s->cv_work.wait_for(lock, std::chrono::milliseconds(2), has_work);
             if (s->stopping) {
-                // Let the launched epochs finish (no kernel may touch memory
-                // that is about to be freed), then cancel everything else.
+                // Wait for the planner to stop and for the launched epochs to
+                // finish (no kernel may touch memory that is about to be
+                // freed), then cancel everything not yet completed.
+                s->cv_work.wait(lock, [&] { return s->planner_done; });
                 lock.unlock();
                 for (EpochSlot& e : s->slots) retire_slot(s, e);
                 lock.lock();
@@ -383,19 +468,22 @@ void worker_loop(xk_server* s) {
                     s->pending.pop_front();
                     finish_request(s, q, XK_ERR_SHUTDOWN);
                 }
-                for (Req* q : s->active) {
-                    q->status = XK_ERR_SHUTDOWN;
-                    q->state = ReqState::Computed;
-                    s->computed.push_back(q);
+                while (!s->to_plan.empty()) {
+                    Req* q = s->to_plan.front();
+                    s->to_plan.pop_front();
+                    auto it = std::find(s->active.begin(), s->active.end(), q);
+                    if (it != s->active.end()) s->active.erase(it);
+                    s->used_bytes -= q->bytes;
+                    finish_request(s, q, XK_ERR_SHUTDOWN);
                 }
-                s->active.clear();
+                for (Req* q : std::vector<Req*>(s->active)) to_computed(s, q, XK_ERR_SHUTDOWN);
+                s->worker_done = true;
                 s->cv_work.notify_all();
                 break;
             }
             // Admission: FIFO while the budget and the slot count allow.
-            while (!s->pending.empty() && (int)s->active.size() < s->opts.max_active) {
+            while (can_admit()) {
                 Req* q = s->pending.front();
-                if (s->used_bytes + q->bytes > s->opts.hbm_budget_bytes && !s->active.empty()) break;
                 s->pending.pop_front();
                 if (q->bytes > s->opts.hbm_budget_bytes) {
                     finish_request(s, q, XK_ERR_BUDGET);
@@ -406,35 +494,9 @@ void worker_loop(xk_server* s) {
                 q->state = ReqState::Admitted;
                 q->t_admit = Clock::now();
                 s->active.push_back(q);
-                admitted.push_back(q);
+                s->to_plan.push_back(q);
+                s->cv_plan.notify_all();
             }
-        }
-        for (Req* q : admitted) {
-            xk::Status st = setup_request(s, q);
-            q->t_planned = Clock::now();
-            std::lock_guard<std::mutex> lock(s->mu);
-            if (!st.ok()) {
-                s->last_error = st.msg;
-                cudaGetLastError();
-                q->status = st.code;
-                q->state = ReqState::Computed;
-                s->active.erase(std::find(s->active.begin(), s->active.end(), q));
-                s->computed.push_back(q);
-                s->cv_work.notify_all();
-                continue;
-            }
-            if (q->routed) {
-                q->state = ReqState::Computed;
-                s->active.erase(std::find(s->active.begin(), s->active.end(), q));
-                s->computed.push_back(q);
-                s->cv_work.notify_all();
-            } else {
-                q->state = ReqState::Running;
-            }
-        }
-        std::vector<Req*> runnable;
-        {
-            std::lock_guard<std::mutex> lock(s->mu);
             for (Req* q : s->active)
                 if (q->state == ReqState::Running && q->next_item < q->n_items) runnable.push_back(q);
         }
@@ -447,17 +509,9 @@ void worker_loop(xk_server* s) {
         }
         std::lock_guard<std::mutex> lock(s->mu);
         if (!st.ok()) s->last_error = st.msg;
-        for (Req* q : runnable) {
-            if (q->next_item >= q->n_items || !st.ok()) {
-                if (!st.ok()) q->status = st.code;
-                q->state = ReqState::Computed;
-                s->active.erase(std::find(s->active.begin(), s->active.end(), q));
-                s->computed.push_back(q);
-            }
-        }
-        s->cv_work.notify_all();
+        for (Req* q : runnable)
+            if (q->next_item >= q->n_items || !st.ok()) to_computed(s, q, st.ok() ? XK_OK : st.code);
     }
-    for (EpochSlot& e : s->slots) retire_slot(s, e);
 }
 
 void finisher_loop(xk_server* s) {
@@ -467,9 +521,9 @@ void finisher_loop(xk_server* s) {
         {
             std::unique_lock<std::mutex> lock(s->mu);
             s->cv_work.wait_for(lock, std::chrono::milliseconds(2),
-                                [&] { return !s->computed.empty() || s->stopping; });
+                                [&] { return !s->computed.empty() || s->worker_done; });
             if (s->computed.empty()) {
-                if (s->stopping && s->active.empty() && s->pending.empty()) break;
+                if (s->worker_done) break;
                 continue;
             }
             q = s->computed.front();
@@ -486,9 +540,16 @@ void finisher_loop(xk_server* s) {
             double* dst[4] = {h.es_re, h.es_im, h.ep_re, h.ep_im};
             const double* src[4] = {q->in.out.es_re, q->in.out.es_im, q->in.out.ep_re, q->in.out.ep_im};
             for (int f = 0; f < 4; ++f)
-                if (cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyDeviceToHost, s->io_stream) != cudaSuccess)
+                if (cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyDeviceToHost, s->out_stream) != cudaSuccess)
                     status = XK_ERR_CUDA;
-            if (cudaStreamSynchronize(s->io_stream) != cudaSuccess) status = XK_ERR_CUDA;
+            if (cudaStreamSynchronize(s->out_stream) != cudaSuccess) status = XK_ERR_CUDA;
+        }
+        if (status != XK_OK) {
+            // A failed request may still have planning or FP64 work queued on
+            // its memory: let it drain before the memory is freed.
+            cudaStreamSynchronize(s->plan_stream);
+            cudaStreamSynchronize(s->f64_stream);
+            cudaGetLastError();
         }
         release_request_memory(s, q);
         std::lock_guard<std::mutex> lock(s->mu);
@@ -500,8 +561,12 @@ void destroy_server(xk_server* s) {
     {
         std::lock_guard<std::mutex> lock(s->mu);
         s->stopping = true;
+        if (!s->planner.joinable()) s->planner_done = true;
+        if (!s->worker.joinable()) s->worker_done = true;
     }
     s->cv_work.notify_all();
+    s->cv_plan.notify_all();
+    if (s->planner.joinable()) s->planner.join();
     if (s->worker.joinable()) s->worker.join();
     if (s->finisher.joinable()) s->finisher.join();
     cudaSetDevice(s->ctx->device);
@@ -512,15 +577,21 @@ void destroy_server(xk_server* s) {
         if (e.h_table) cudaFreeHost(e.h_table);
         if (e.h_err) cudaFreeHost(e.h_err);
     }
-    for (auto& kv : s->reqs) delete kv.second;
-    for (void* p : s->pinned_all) cudaFreeHost(p);
+    for (auto& kv : s->reqs) {
+        Req* q = kv.second;
+        q->arena.release();
+        q->mem.release();
+        if (q->done_ev) cudaEventDestroy(q->done_ev);
+        delete q;
+    }
     for (auto& kv : s->raysets) {
         kv.second->buf.release();
         delete kv.second;
     }
+    s->plan_ws.release();
     s->f64ws.rays.release();
     s->f64ws.partials.release();
-    for (cudaStream_t st : {s->plan_stream, s->exec_stream, s->io_stream, s->f64_stream})
+    for (cudaStream_t st : {s->plan_stream, s->exec_stream, s->io_stream, s->f64_stream, s->out_stream})
         if (st) {
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
@@ -538,6 +609,8 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
     if (s->opts.epoch_pairs <= 0) s->opts.epoch_pairs = 2e10;
     if (s->opts.max_active <= 0) s->opts.max_active = 64;
     if (s->opts.item_pairs <= 0) s->opts.item_pairs = 4e6;
+    if (s->opts.reserve_sms <= 0) s->opts.reserve_sms = 8;
+    s->opts.reserve_sms = std::min(s->opts.reserve_sms, s->num_sms - 1);
     s->pr_opts = ctx->pr_opts;
     // Keep freed stream-ordered memory in the pool instead of returning it to
     // the driver at every synchronisation.
@@ -551,6 +624,7 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
     XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->exec_stream, cudaStreamNonBlocking, lo));
     XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->io_stream, cudaStreamNonBlocking, hi));
     XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->f64_stream, cudaStreamNonBlocking, lo));
+    XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->out_stream, cudaStreamNonBlocking, hi));
     for (EpochSlot& e : s->slots) {
         XK_TRY(e.table.ensure(kVariants * (size_t)std::max(1, s->opts.max_active) * sizeof(xk::PrSolve)));
         XK_TRY(e.ctrl.ensure(256));
@@ -560,15 +634,14 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
         *e.h_err = 0;
         XK_CUDA_TRY(cudaEventCreateWithFlags(&e.ev, cudaEventDisableTiming));
     }
-    for (int i = 0; i < s->opts.max_active; ++i) {
-        void* p = nullptr;
-        XK_CUDA_TRY(cudaMallocHost(&p, kPinnedBlock));
-        s->pinned_all.push_back(p);
-        s->pinned_free.push_back(p);
-    }
+    // The planner's scratch: CUB temporaries grow stream-ordered; the pinned
+    // readback area is sized once for the largest planning batch.
+    s->plan_ws.set_async(s->plan_stream);
+    XK_TRY(xk::pr_reserve_plan_host(s->plan_ws, kPlanBatch, s->num_sms));
     s->f64ws.rays.async_stream = s->f64_stream;
     s->f64ws.partials.async_stream = s->f64_stream;
     s->worker = std::thread(worker_loop, s);
+    s->planner = std::thread(planner_loop, s);
     s->finisher = std::thread(finisher_loop, s);
     return xk::Status::Ok();
 }
@@ -612,20 +685,19 @@ int xk_server_upload_rays(xk_server* s, const xk_rays* rays, size_t n, uint64_t*
     cudaSetDevice(s->ctx->device);
     RaySet* rs = new RaySet();
     rs->n = n;
+    rs->buf.async_stream = s->io_stream;
     const double* src[12] = {rays->x, rays->y, rays->z, rays->nx, rays->ny, rays->nz, rays->nl,
                              rays->es_re, rays->es_im, rays->ep_re, rays->ep_im, rays->energy};
     int rc = XK_OK;
-    cudaStream_t st = nullptr;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) rc = XK_ERR_CUDA;
-    if (rc == XK_OK && !rs->buf.ensure(12 * n * sizeof(double)).ok()) rc = XK_ERR_OOM;
+    cudaStream_t st = s->io_stream;
+    if (!rs->buf.ensure(12 * n * sizeof(double)).ok()) rc = XK_ERR_OOM;
     for (int f = 0; f < 12 && rc == XK_OK; ++f)
         if (cudaMemcpyAsync(rs->buf.as<double>() + f * n, src[f], n * 8, cudaMemcpyHostToDevice, st) !=
             cudaSuccess)
             rc = XK_ERR_CUDA;
-    if (st) {
-        if (cudaStreamSynchronize(st) != cudaSuccess && rc == XK_OK) rc = XK_ERR_CUDA;
-        cudaStreamDestroy(st);
-    }
+    // Requests that use the set are planned on other streams: the set must be
+    // complete before this call returns.
+    if (cudaStreamSynchronize(st) != cudaSuccess && rc == XK_OK) rc = XK_ERR_CUDA;
     std::lock_guard<std::mutex> lock(s->mu);
     if (rc != XK_OK) {
         s->used_bytes -= bytes;

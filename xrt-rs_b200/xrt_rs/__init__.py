@@ -27,6 +27,7 @@ __all__ = [
     "diffraction_integral_rs", "diffraction_integral", "diffraction_integral_device",
     "GpuContext", "kirchhoff_gpu", "kirchhoff_auto", "GPU_RAY_DTYPE", "GPU_PIXEL_DTYPE",
     "XkError", "XK_PATH_F64", "XK_PATH_F32PR", "RAY_FIELDS", "PIXEL_FIELDS", "Batch",
+    "autotune",
 ]
 
 RAY_FIELDS = ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re", "ep_im", "energy")
@@ -299,6 +300,28 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def autotune(rays, pixels, out, ctx=None, budget_ms=3000.0, apply=True):
+    """Tune the FP32-PR knobs on a device-resident problem (tensors with
+    ``data_ptr()``); keeps the fastest settings on ``ctx`` when ``apply``."""
+    ctx = _require_ctx(ctx)
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def cast(t):
+        return ctypes.cast(ctypes.c_void_p(int(t.data_ptr())), dp)
+
+    if isinstance(rays, dict):
+        rays = [rays[k] for k in RAY_FIELDS]
+    if isinstance(pixels, dict):
+        pixels = [pixels[k] for k in PIXEL_FIELDS]
+    res = _lib.XkTuneResult()
+    rc = _lib.load().xk_autotune(ctx.handle, _lib.XkRays(*[cast(a) for a in rays]),
+                                 int(rays[0].numel()), _lib.XkPixels(*[cast(a) for a in pixels]),
+                                 int(pixels[0].numel()), _lib.XkField(*[cast(a) for a in out]),
+                                 float(budget_ms), 1 if apply else 0, ctypes.byref(res))
+    _lib.check(rc, ctx.handle)
+    return res.to_dict()
 
 
 def _as_records(a, dtype):

@@ -99,6 +99,15 @@ class XkSolvePlan(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class XkTuneResult(ctypes.Structure):
+    _fields_ = [("default_ms", ctypes.c_double), ("best_ms", ctypes.c_double),
+                ("phase_budget", ctypes.c_double), ("items_per_warp", ctypes.c_longlong),
+                ("sweep", ctypes.c_int), ("trials", ctypes.c_int)]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 XK_BATCH_DEVICE = 1
 XK_BATCH_NO_GRAPH = 2
 
@@ -106,7 +115,7 @@ XK_BATCH_NO_GRAPH = 2
 class XkServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_double), ("epoch_pairs", ctypes.c_double),
                 ("max_active", ctypes.c_int), ("item_pairs", ctypes.c_double),
-                ("inject_alloc_failure_every", ctypes.c_int)]
+                ("inject_alloc_failure_every", ctypes.c_int), ("reserve_sms", ctypes.c_int)]
 
 
 class XkRequest(ctypes.Structure):
@@ -158,6 +167,10 @@ _SIGNATURES = {
     "xk_diffraction_f64_noalloc": (ctypes.c_int, [
         ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels), ctypes.c_size_t,
         ctypes.POINTER(XkField), ctypes.c_void_p]),
+    "xk_autotune": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels),
+        ctypes.c_size_t, ctypes.POINTER(XkField), ctypes.c_double, ctypes.c_int,
+        ctypes.POINTER(XkTuneResult)]),
     "xk_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkSolve), ctypes.c_size_t,
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "xk_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkBatchStats)]),

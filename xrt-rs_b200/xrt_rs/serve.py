@@ -20,10 +20,11 @@ from . import (PIXEL_FIELDS, RAY_FIELDS, XkError, _check_lengths, _f64, _path, _
 
 class Server:
     def __init__(self, ctx=None, hbm_budget_bytes=0.0, epoch_pairs=0.0, max_active=0,
-                 item_pairs=0.0, inject_alloc_failure_every=0):
+                 item_pairs=0.0, inject_alloc_failure_every=0, reserve_sms=0):
         self._ctx = _require_ctx(ctx)
         opts = _lib.XkServerOpts(float(hbm_budget_bytes), float(epoch_pairs), int(max_active),
-                                 float(item_pairs), int(inject_alloc_failure_every))
+                                 float(item_pairs), int(inject_alloc_failure_every),
+                                 int(reserve_sms))
         h = ctypes.c_void_p()
         _lib.check(_lib.load().xk_server_create(self._ctx.handle, ctypes.byref(opts),
                                                 ctypes.byref(h)), self._ctx.handle)
