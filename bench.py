@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sweep", type=int, default=-1, help="-1 auto, 0 SFU reciprocal, 1 packed")
-    ap.add_argument("--phase-budget", type=float, default=256.0)
+    ap.add_argument("--phase-budget", type=float, default=512.0)
     ap.add_argument("--workload", choices=["single", "batch", "sweep", "serve"], default="single",
                     help="single: the 2^20 x 512^2 solve (default); batch: 64 uneven solves; "
                          "sweep: the energy x distance precision sweep")

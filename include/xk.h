@@ -141,7 +141,7 @@ const char* xk_route_reason(int reason);
 
 /* Tuning knobs of the F32PR path (no counterpart in the reference, whose
  * shader has no parameters). Names:
- *   "phase_budget"   bound on the FP32 residual phase in rad (default 256)
+ *   "phase_budget"   bound on the FP32 residual phase in rad (default 512)
  *   "sweep"          -1 automatic, 0 SFU reciprocal, 1 packed f32x2 sweep
  *   "groups"         ray ranges per screen tile, 0 = automatic
  *   "items_per_warp" target work items per resident warp (automatic groups) */
@@ -196,6 +196,59 @@ int xk_kirchhoff_gpu(xk_ctx* ctx, const xk_gpu_ray* rays, size_t n_rays,
  * returns XK_ERR_NO_DEVICE. */
 int xk_kirchhoff_auto(const xk_gpu_ray* rays, size_t n_rays, const xk_gpu_pixel* pixels,
                       size_t n_pix, double* out);
+
+/* ---- screens and rays from a beam -----------------------------------------
+ *
+ * The two producers in front of the path (src/waves/prepare_wave.rs), run on
+ * the device so that a beam's columns go to the GPU once and neither the
+ * screen grid nor the ray records make a host round trip. */
+
+/* WaveParams (src/waves/prepare_wave.rs:11-23). */
+typedef struct xk_wave_params {
+    double center[3]; /* screen centre [mm] */
+    double dx, dz;    /* half-widths in x and z [mm] */
+    size_t nx, nz;    /* points along x and along z */
+} xk_wave_params;
+
+/* The columns of core::beam::Beam that beam_to_diffraction_rays reads, one
+ * f64 per beam ray in each array. The four amplitude arrays are either all
+ * set or all NULL (a beam without amplitudes: es = 1, ep = 0). */
+typedef struct xk_beam {
+    const double *x, *y, *z;  /* position [mm] */
+    const double *a, *b, *c;  /* direction cosines */
+    const double *e;          /* energy [eV] */
+    const double *es_re, *es_im, *ep_re, *ep_im;
+} xk_beam;
+
+/* Writable ray and screen-point arrays (outputs of the two producers). */
+typedef struct xk_rays_out {
+    double *x, *y, *z, *nx, *ny, *nz, *nl, *es_re, *es_im, *ep_re, *ep_im, *energy;
+} xk_rays_out;
+typedef struct xk_pixels_out {
+    double *x, *y, *z;
+} xk_pixels_out;
+
+/* prepare_wave (src/waves/prepare_wave.rs:40-68): the nx*nz screen points,
+ * x outer and z inner (index ix*nz + iz), y = center[1], computed on the
+ * device with the reference's operation order; `out` holds host arrays of
+ * nx*nz doubles. nx*nz == 0 is a no-op. */
+int xk_prepare_wave(xk_ctx* ctx, const xk_wave_params* params, xk_pixels_out* out);
+
+/* beam_to_diffraction_rays (src/waves/prepare_wave.rs:78-111): ray i is beam
+ * ray good[i] with its surface normal normals[3*good[i] .. +3] and
+ * nl = n.(a, b, c); `beam` and `normals` (n_beam rows of 3 doubles) are host
+ * arrays, `out` holds host arrays of n_good doubles. A good index >= n_beam
+ * returns XK_ERR_INVALID (the reference panics). */
+int xk_beam_to_rays(xk_ctx* ctx, const xk_beam* beam, size_t n_beam, const double* normals,
+                    const size_t* good, size_t n_good, xk_rays_out* out);
+
+/* The whole chain on the device: uploads the beam's columns, builds the rays
+ * of `good` and the screen of `params` in HBM and solves the integral on them
+ * (as xk_diffraction_integral, whose result it equals bit for bit). `out`
+ * holds host arrays of params->nx * params->nz doubles. */
+int xk_diffraction_beam(xk_ctx* ctx, const xk_beam* beam, size_t n_beam, const double* normals,
+                        const size_t* good, size_t n_good, const xk_wave_params* params,
+                        xk_field* out, int path, xk_stats* stats);
 
 /* ---- batches of solves ------------------------------------------------------
  *

@@ -31,6 +31,14 @@
  *                      then the f64 base-phase restore with the mean energy.
  *                      It measures the reference GPU algorithm's own error.
  *
+ * And the producers and the sibling sum around the path:
+ *
+ *   oracle_prepare_wave  src/waves/prepare_wave.rs:40-68 (screen grid, x outer).
+ *   oracle_beam_rays     src/waves/prepare_wave.rs:78-111 (beam -> rays, nl = n.dir).
+ *   oracle_fresnel       src/waves/fresnel.rs:53-106 (2-D Fresnel sum
+ *                        U = sum_j es_j exp(i k/(2d) |p - r_j|^2) over a grid,
+ *                        z outer, plain complex accumulation).
+ *
  * Pixels run in parallel (OpenMP), mirroring the reference's Rayon
  * `par_iter` over pixels (src/waves/diffraction.rs:60-63); each pixel's ray
  * loop is sequential, so results do not depend on the thread count.
@@ -289,5 +297,91 @@ void oracle_wgsl_f32(const float* rx, const float* ry, const float* rz,
         cplx es = {(double)a_re, (double)a_im}, ep = {(double)b_re, (double)b_im};
         cplx r1 = c_mul(es, ph), r2 = c_mul(ep, ph);
         o_es_re[i] = r1.re; o_es_im[i] = r1.im; o_ep_re[i] = r2.re; o_ep_im[i] = r2.im;
+    }
+}
+
+
+/* ---- screen grid (src/waves/prepare_wave.rs:40-68) ---------------------- */
+
+static double grid_frac(size_t i, size_t n) {
+    return n > 1 ? (double)i / (double)(n - 1) - 0.5 : 0.0;
+}
+
+void oracle_prepare_wave(const double* center, double dx, double dz, size_t nx, size_t nz,
+                         double* px, double* py, double* pz) {
+    for (size_t ix = 0; ix < nx; ++ix) {
+        double x = center[0] + grid_frac(ix, nx) * 2.0 * dx;
+        for (size_t iz = 0; iz < nz; ++iz) {
+            size_t i = ix * nz + iz;
+            px[i] = x;
+            py[i] = center[1];
+            pz[i] = center[2] + grid_frac(iz, nz) * 2.0 * dz;
+        }
+    }
+}
+
+/* ---- beam -> rays (src/waves/prepare_wave.rs:78-111) --------------------
+ * beam: 7 columns (x, y, z, a, b, c, e) then 4 amplitude columns or NULLs;
+ * normals: n_beam rows of 3; out: the 12 ray columns. */
+void oracle_beam_rays(const double* const* beam, const double* normals, const size_t* good,
+                      size_t n_good, double* const* out) {
+    for (size_t i = 0; i < n_good; ++i) {
+        size_t j = good[i];
+        const double* n = normals + 3 * j;
+        out[0][i] = beam[0][j];
+        out[1][i] = beam[1][j];
+        out[2][i] = beam[2][j];
+        out[3][i] = n[0];
+        out[4][i] = n[1];
+        out[5][i] = n[2];
+        out[6][i] = n[0] * beam[3][j] + n[1] * beam[4][j] + n[2] * beam[5][j];
+        if (beam[7]) {
+            out[7][i] = beam[7][j];
+            out[8][i] = beam[8][j];
+            out[9][i] = beam[9][j];
+            out[10][i] = beam[10][j];
+        } else {
+            out[7][i] = 1.0;
+            out[8][i] = 0.0;
+            out[9][i] = 0.0;
+            out[10][i] = 0.0;
+        }
+        out[11][i] = beam[6][j];
+    }
+}
+
+/* ---- 2-D Fresnel sum (src/waves/fresnel.rs:53-106) ----------------------
+ * Screen coordinates x_i = x_min + (x_max - x_min) * i / max(nx - 1, 1)
+ * (same for z); output index iz * nx + ix; per term
+ * es_j * exp((0, k/(2d)) * r2) with the complex exponential of a purely
+ * imaginary argument (cos, sin), textbook complex multiply, plain sum. */
+void oracle_fresnel(const double* rx, const double* rz, const double* es_re, const double* es_im,
+                    size_t n, double energy, double dist, double x_min, double x_max, size_t nx,
+                    double z_min, double z_max, size_t nz, double* o_re, double* o_im,
+                    int n_threads) {
+    set_threads(n_threads);
+    const double k = energy / ORACLE_CHBAR * 1e7;
+    const double pre_im = k / (2.0 * dist);
+    const double xden = (double)(nx > 1 ? nx - 1 : 1), zden = (double)(nz > 1 ? nz - 1 : 1);
+    long long total = (long long)(nx * nz);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long long idx = 0; idx < total; ++idx) {
+        size_t iz = (size_t)idx / nx, ix = (size_t)idx - iz * nx;
+        double xp = x_min + (x_max - x_min) * (double)ix / xden;
+        double zp = z_min + (z_max - z_min) * (double)iz / zden;
+        double s_re = 0.0, s_im = 0.0;
+        for (size_t j = 0; j < n; ++j) {
+            double dx = xp - rx[j];
+            double dz = zp - rz[j];
+            double r2 = dx * dx + dz * dz;
+            double th = pre_im * r2;
+            cplx ph = {cos(th), sin(th)};
+            cplx e = {es_re[j], es_im[j]};
+            cplx t = c_mul(e, ph);
+            s_re += t.re;
+            s_im += t.im;
+        }
+        o_re[idx] = s_re;
+        o_im[idx] = s_im;
     }
 }

@@ -150,3 +150,28 @@ def rel_l2_intensity(out, ref):
     ib = np.abs(eb) ** 2 + np.abs(pb) ** 2
     den = np.linalg.norm(ib)
     return float(np.linalg.norm(ia - ib) / den) if den > 0 else float(np.linalg.norm(ia - ib))
+
+
+def beam_case(n, seed, amplitudes=True, dist_y=2000.0):
+    """A seeded beam after a mirror, in the column layout beam_to_diffraction_rays
+    reads (x, y, z, a, b, c, e, es/ep), with per-ray normals and a `good`
+    subset in shuffled order with repeats — the shape of
+    tests/pipeline.rs:13-54 (source -> flat mirror -> screen at y = 2000)."""
+    rng = np.random.default_rng(seed)
+    d = rng.normal(0, 1e-4, (n, 3))
+    d[:, 1] += 1.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    beam = {"x": rng.normal(0, 0.1, n), "y": rng.normal(0, 1e-3, n), "z": rng.normal(0, 0.1, n),
+            "a": d[:, 0].copy(), "b": d[:, 1].copy(), "c": d[:, 2].copy(),
+            "e": np.full(n, 10000.0)}
+    if amplitudes:
+        es = rng.uniform(0.5, 1.0, n) * np.exp(1j * rng.uniform(-0.3, 0.3, n))
+        ep = 0.1 * es
+        beam.update(es_re=es.real.copy(), es_im=es.imag.copy(), ep_re=ep.real.copy(),
+                    ep_im=ep.imag.copy())
+    nrm = rng.normal(0, 0.02, (n, 3))
+    nrm[:, 1] += 1.0
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    good = rng.permutation(n)[: max(1, (9 * n) // 10)]
+    good = np.concatenate([good, good[:3]])  # repeats are allowed
+    return beam, nrm, good.astype(np.uint64)

@@ -5,7 +5,9 @@
 // host buffers stage them through device buffers the context keeps and
 // grows, so repeated calls of the same size allocate nothing.
 
+#include <algorithm>
 #include <chrono>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -62,6 +64,7 @@ void destroy_ctx(xk_ctx* ctx) {
     ctx->in_rays.release();
     ctx->in_pix.release();
     ctx->out_field.release();
+    ctx->in_beam.release();
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -175,6 +178,69 @@ xk::Status solve_host(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_
     return finish_stats(ctx, stats, used, n_rays, n_pix);
 }
 
+
+// ---- screen grid and beam producers ---------------------------------------
+
+static_assert(sizeof(size_t) == sizeof(uint64_t), "good indices are copied as 64-bit words");
+
+bool beam_ok(const xk_beam* b) {
+    if (!b || !b->x || !b->y || !b->z || !b->a || !b->b || !b->c || !b->e) return false;
+    const int amps = !!b->es_re + !!b->es_im + !!b->ep_re + !!b->ep_im;
+    return amps == 0 || amps == 4;
+}
+
+xk::Status wave_size(const xk_wave_params* p, size_t* m) {
+    if (p->nx && p->nz > SIZE_MAX / p->nx)
+        return xk::Status::Err(XK_ERR_INVALID, "nx * nz overflows");
+    *m = p->nx * p->nz;
+    return xk::Status::Ok();
+}
+
+xk::WaveGrid to_grid(const xk_wave_params* p) {
+    return xk::WaveGrid{p->center[0], p->center[1], p->center[2], p->dx, p->dz, p->nx, p->nz};
+}
+
+// Uploads the beam columns, normals and good indices into ctx->in_beam.
+xk::Status upload_beam(xk_ctx* ctx, const xk_beam* beam, size_t n_beam, const double* normals,
+                       const size_t* good, size_t n_good, cudaStream_t s, xk::BeamDev* bd,
+                       const uint64_t** d_good, double* h2d) {
+    for (size_t i = 0; i < n_good; ++i)
+        if (good[i] >= n_beam) return xk::Status::Err(XK_ERR_INVALID, "good index out of range");
+    const bool amps = beam->es_re != nullptr;
+    const int cols = amps ? 11 : 7;
+    const size_t nb = n_beam * sizeof(double);
+    const size_t bytes = (size_t)cols * nb + 3 * nb + n_good * sizeof(uint64_t);
+    XK_TRY(ctx->in_beam.ensure(std::max<size_t>(bytes, 8)));
+    double* d = ctx->in_beam.as<double>();
+    const double* src[11] = {beam->x, beam->y, beam->z, beam->a, beam->b, beam->c, beam->e,
+                             beam->es_re, beam->es_im, beam->ep_re, beam->ep_im};
+    const double** dst = reinterpret_cast<const double**>(bd);
+    *bd = xk::BeamDev{};
+    for (int f = 0; f < cols; ++f) {
+        dst[f] = d;
+        if (n_beam) XK_CUDA_TRY(cudaMemcpyAsync(d, src[f], nb, cudaMemcpyHostToDevice, s));
+        d += n_beam;
+    }
+    bd->normals = d;
+    if (n_beam) XK_CUDA_TRY(cudaMemcpyAsync(d, normals, 3 * nb, cudaMemcpyHostToDevice, s));
+    d += 3 * n_beam;
+    *d_good = reinterpret_cast<const uint64_t*>(d);
+    if (n_good)
+        XK_CUDA_TRY(cudaMemcpyAsync(d, good, n_good * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    *h2d = (double)bytes;
+    return xk::Status::Ok();
+}
+
+// Device columns of the ray staging buffer (12 x n).
+void ray_columns(xk_ctx* ctx, size_t n, double* cols[12], xk::RaysDev* rd) {
+    double* d = ctx->in_rays.as<double>();
+    const double** f = reinterpret_cast<const double**>(rd);
+    for (int i = 0; i < 12; ++i) {
+        cols[i] = d + i * n;
+        f[i] = cols[i];
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -282,8 +348,8 @@ int xk_autotune(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_pixels
         int sweep;
     };
     const Cand cands[] = {{base.phase_budget, base.items_per_warp, base.sweep},
-                          {512.0, 16, -1}, {128.0, 16, -1}, {256.0, 32, -1}, {256.0, 8, -1},
-                          {512.0, 32, -1}, {512.0, 8, -1}, {256.0, 16, 0}, {512.0, 16, 0}};
+                          {512.0, 32, -1}, {512.0, 8, -1}, {256.0, 16, -1}, {384.0, 16, -1},
+                          {512.0, 16, 0}, {256.0, 32, -1}, {256.0, 8, -1}, {128.0, 16, -1}};
     double spent = 0.0, best = 1e300;
     xk::PrOptions best_opt = base;
     int trials = 0;
@@ -414,6 +480,127 @@ int xk_kirchhoff_auto(const xk_gpu_ray* rays, size_t n_rays, const xk_gpu_pixel*
     int rc = xk_shared(&ctx);
     if (rc != XK_OK || !ctx) return rc == XK_OK ? XK_ERR_NO_DEVICE : rc;
     return xk_kirchhoff_gpu(ctx, rays, n_rays, pixels, n_pix, out);
+}
+
+int xk_prepare_wave(xk_ctx* ctx, const xk_wave_params* params, xk_pixels_out* out) {
+    if (!ctx) return XK_ERR_INVALID;
+    if (!params) return fail(ctx, XK_ERR_INVALID, "null wave parameters");
+    size_t m = 0;
+    xk::Status st = wave_size(params, &m);
+    if (!st.ok()) return fail(ctx, st);
+    if (m == 0) return XK_OK;
+    if (!out || !out->x || !out->y || !out->z)
+        return fail(ctx, XK_ERR_INVALID, "null array pointer");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const size_t mb = m * sizeof(double);
+    st = ctx->in_pix.ensure(3 * mb);
+    if (st.ok()) {
+        double* d = ctx->in_pix.as<double>();
+        st = xk::wave_enqueue(to_grid(params), d, d + m, d + 2 * m, s);
+        double* dst[3] = {out->x, out->y, out->z};
+        for (int f = 0; f < 3 && st.ok(); ++f)
+            if (cudaMemcpyAsync(dst[f], d + f * m, mb, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+                st = xk::Status::Err(XK_ERR_CUDA, "device-to-host copy failed");
+        if (st.ok() && cudaStreamSynchronize(s) != cudaSuccess)
+            st = xk::Status::Err(XK_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    }
+    return st.ok() ? XK_OK : fail(ctx, st);
+}
+
+int xk_beam_to_rays(xk_ctx* ctx, const xk_beam* beam, size_t n_beam, const double* normals,
+                    const size_t* good, size_t n_good, xk_rays_out* out) {
+    if (!ctx) return XK_ERR_INVALID;
+    if (n_good == 0) return XK_OK;
+    bool out_ok = out != nullptr;
+    if (out_ok) {
+        double* h[12] = {out->x, out->y, out->z, out->nx, out->ny, out->nz, out->nl,
+                         out->es_re, out->es_im, out->ep_re, out->ep_im, out->energy};
+        for (double* p : h) out_ok = out_ok && p;
+    }
+    if (!beam_ok(beam) || !normals || !good || !out_ok)
+        return fail(ctx, XK_ERR_INVALID, "null array pointer (or amplitudes only partly set)");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    xk::BeamDev bd;
+    const uint64_t* d_good = nullptr;
+    double h2d = 0.0;
+    xk::Status st = upload_beam(ctx, beam, n_beam, normals, good, n_good, s, &bd, &d_good, &h2d);
+    if (st.ok()) st = ctx->in_rays.ensure(12 * n_good * sizeof(double));
+    if (st.ok()) {
+        double* cols[12];
+        xk::RaysDev rd;
+        ray_columns(ctx, n_good, cols, &rd);
+        st = xk::beam_rays_enqueue(bd, d_good, n_good, cols, s);
+        double* h[12] = {out->x, out->y, out->z, out->nx, out->ny, out->nz, out->nl,
+                         out->es_re, out->es_im, out->ep_re, out->ep_im, out->energy};
+        for (int f = 0; f < 12 && st.ok(); ++f)
+            if (cudaMemcpyAsync(h[f], cols[f], n_good * sizeof(double),
+                                cudaMemcpyDeviceToHost, s) != cudaSuccess)
+                st = xk::Status::Err(XK_ERR_CUDA, "device-to-host copy failed");
+        if (st.ok() && cudaStreamSynchronize(s) != cudaSuccess)
+            st = xk::Status::Err(XK_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    }
+    return st.ok() ? XK_OK : fail(ctx, st);
+}
+
+int xk_diffraction_beam(xk_ctx* ctx, const xk_beam* beam, size_t n_beam, const double* normals,
+                        const size_t* good, size_t n_good, const xk_wave_params* params,
+                        xk_field* out, int path, xk_stats* stats) {
+    if (!ctx) return XK_ERR_INVALID;
+    if (!params) return fail(ctx, XK_ERR_INVALID, "null wave parameters");
+    if (path != XK_PATH_F64 && path != XK_PATH_F32PR)
+        return fail(ctx, XK_ERR_INVALID, "unknown path");
+    size_t m = 0;
+    xk::Status st = wave_size(params, &m);
+    if (!st.ok()) return fail(ctx, st);
+    auto t0 = std::chrono::steady_clock::now();
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (m == 0) return XK_OK;
+    if (!field_ok(out) || (n_good && (!beam_ok(beam) || !normals || !good)))
+        return fail(ctx, XK_ERR_INVALID, "null array pointer (or amplitudes only partly set)");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    xk::BeamDev bd;
+    const uint64_t* d_good = nullptr;
+    double h2d = 0.0;
+    if (n_good) st = upload_beam(ctx, beam, n_beam, normals, good, n_good, s, &bd, &d_good, &h2d);
+    if (st.ok()) st = ctx->in_rays.ensure(std::max<size_t>(12 * n_good * sizeof(double), 8));
+    if (st.ok()) st = ctx->in_pix.ensure(3 * m * sizeof(double));
+    if (st.ok()) st = ctx->out_field.ensure(4 * m * sizeof(double));
+    if (!st.ok()) return fail(ctx, st);
+    double* cols[12];
+    xk::RaysDev rd;
+    ray_columns(ctx, n_good, cols, &rd);
+    st = xk::beam_rays_enqueue(bd, d_good, n_good, cols, s);
+    double* dp = ctx->in_pix.as<double>();
+    if (st.ok()) st = xk::wave_enqueue(to_grid(params), dp, dp + m, dp + 2 * m, s);
+    xk::PixDev pd{dp, dp + m, dp + 2 * m};
+    double* dout = ctx->out_field.as<double>();
+    xk::FieldDev fd{dout, dout + m, dout + 2 * m, dout + 3 * m};
+    int used = path;
+    if (st.ok()) st = run_solve(ctx, rd, n_good, pd, m, fd, path, s, stats, &used);
+    double* hdst[4] = {out->es_re, out->es_im, out->ep_re, out->ep_im};
+    for (int i = 0; i < 4 && st.ok(); ++i)
+        if (cudaMemcpyAsync(hdst[i], dout + i * m, m * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess)
+            st = xk::Status::Err(XK_ERR_CUDA, "device-to-host copy failed");
+    if (st.ok() && cudaStreamSynchronize(s) != cudaSuccess)
+        st = xk::Status::Err(XK_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    if (st.ok()) st = finish_stats(ctx, stats, used, n_good, m);
+    if (!st.ok()) return fail(ctx, st);
+    if (stats) {
+        stats->h2d_bytes = h2d;
+        stats->d2h_bytes = 4.0 * m * sizeof(double);
+        stats->kernels += (n_good ? 1 : 0) + 1;
+        stats->wall_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                .count();
+    }
+    return XK_OK;
 }
 
 }  // extern "C"

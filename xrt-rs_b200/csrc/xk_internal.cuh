@@ -107,4 +107,21 @@ Status f64_enqueue(const RaysDev& rays, size_t n_rays, const PixDev& pix, size_t
                    const FieldDev& out, F64Workspace& ws, cudaStream_t stream, int num_sms,
                    LaunchReport* rep);
 
+// Screen grid and beam-to-ray producers (xk_wave.cu), enqueued on `stream`.
+struct WaveGrid {
+    double cx, cy, cz, dx, dz;
+    size_t nx, nz;
+};
+struct BeamDev {
+    const double *x, *y, *z, *a, *b, *c, *e, *es_re, *es_im, *ep_re, *ep_im;  // amplitudes may be null
+    const double* normals;  // n_beam rows of 3
+};
+// Writes nx*nz points into x/y/z (device arrays).
+Status wave_enqueue(const WaveGrid& g, double* x, double* y, double* z, cudaStream_t stream);
+// Gathers the rays of `good` (device array of n_good indices < n_beam) into
+// the 12 device columns of `out` (x, y, z, nx, ny, nz, nl, es_re, es_im,
+// ep_re, ep_im, energy).
+Status beam_rays_enqueue(const BeamDev& beam, const uint64_t* good, size_t n_good,
+                         double* const out[12], cudaStream_t stream);
+
 }  // namespace xk

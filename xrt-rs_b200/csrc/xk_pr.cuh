@@ -15,7 +15,7 @@ constexpr int kPrTile = 32 * kPrPpl;  // screen points per tile (one warp)
 
 // Planner knobs.
 struct PrOptions {
-    double phase_budget = 256.0;  // bound on |FP32 residual phase| [rad]
+    double phase_budget = 512.0;  // bound on |FP32 residual phase| [rad]
     int groups = 0;               // ray groups per tile; 0 = automatic
     int sweep = -1;               // -1 automatic, 0 SFU reciprocal, 1 packed + Newton
     long long items_per_warp = 16;  // target items per resident warp (automatic groups)

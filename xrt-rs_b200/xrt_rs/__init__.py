@@ -27,7 +27,7 @@ __all__ = [
     "diffraction_integral_rs", "diffraction_integral", "diffraction_integral_device",
     "GpuContext", "kirchhoff_gpu", "kirchhoff_auto", "GPU_RAY_DTYPE", "GPU_PIXEL_DTYPE",
     "XkError", "XK_PATH_F64", "XK_PATH_F32PR", "RAY_FIELDS", "PIXEL_FIELDS", "Batch",
-    "autotune",
+    "autotune", "WaveParams", "prepare_wave", "beam_to_diffraction_rays", "diffraction_from_beam",
 ]
 
 RAY_FIELDS = ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re", "ep_im", "energy")
@@ -359,3 +359,7 @@ def kirchhoff_auto(rays, pixels):
                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     _lib.check(rc)
     return out[:, 0] + 1j * out[:, 1], out[:, 2] + 1j * out[:, 3]
+
+
+from .waves import (WaveParams, prepare_wave, beam_to_diffraction_rays,  # noqa: E402
+                    diffraction_from_beam)

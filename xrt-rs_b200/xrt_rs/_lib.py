@@ -143,6 +143,24 @@ class XkServerStats(ctypes.Structure):
     def to_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
+class XkWaveParams(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_double * 3), ("dx", ctypes.c_double), ("dz", ctypes.c_double),
+                ("nx", ctypes.c_size_t), ("nz", ctypes.c_size_t)]
+
+
+class XkBeam(ctypes.Structure):
+    _fields_ = [(n, _dp) for n in ("x", "y", "z", "a", "b", "c", "e",
+                                   "es_re", "es_im", "ep_re", "ep_im")]
+
+
+class XkRaysOut(ctypes.Structure):
+    _fields_ = XkRays._fields_
+
+
+class XkPixelsOut(ctypes.Structure):
+    _fields_ = XkPixels._fields_
+
+
 # Every entry point include/xk.h declares, with its ctypes signature.
 _SIGNATURES = {
     "xk_init": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
@@ -188,6 +206,15 @@ _SIGNATURES = {
                                        ctypes.POINTER(XkRequestStats)]),
     "xk_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkServerStats)]),
     "xk_server_destroy": (None, [ctypes.c_void_p]),
+    "xk_prepare_wave": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkWaveParams),
+                                        ctypes.POINTER(XkPixelsOut)]),
+    "xk_beam_to_rays": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.POINTER(XkBeam), ctypes.c_size_t, _dp,
+        ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t, ctypes.POINTER(XkRaysOut)]),
+    "xk_diffraction_beam": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.POINTER(XkBeam), ctypes.c_size_t, _dp,
+        ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t, ctypes.POINTER(XkWaveParams),
+        ctypes.POINTER(XkField), ctypes.c_int, ctypes.POINTER(XkStats)]),
     "xk_kirchhoff_auto": (ctypes.c_int, [
         ctypes.POINTER(XkGpuRay), ctypes.c_size_t, ctypes.POINTER(XkGpuPixel), ctypes.c_size_t,
         _dp]),
