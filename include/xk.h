@@ -55,7 +55,7 @@ enum {
     XK_ERR_SHUTDOWN = 9   /* server is shutting down */
 };
 
-enum { XK_PATH_F64 = 0, XK_PATH_F32PR = 1 };
+enum { XK_PATH_F64 = 0, XK_PATH_F32PR = 1, XK_PATH_SEPARABLE = 2 };
 
 /* ---- data structures --------------------------------------------------- */
 
@@ -144,7 +144,9 @@ const char* xk_route_reason(int reason);
  *   "phase_budget"   bound on the FP32 residual phase in rad (default 512)
  *   "sweep"          -1 automatic, 0 SFU reciprocal, 1 packed f32x2 sweep
  *   "groups"         ray ranges per screen tile, 0 = automatic
- *   "items_per_warp" target work items per resident warp (automatic groups) */
+ *   "items_per_warp" target work items per resident warp (automatic groups)
+ *   "fresnel_chunk_rays" cap on rays per chunk of the separable Fresnel
+ *                    product (0 = sized by its 2 GiB factor budget) */
 int xk_set_option(xk_ctx* ctx, const char* name, double value);
 
 typedef struct xk_tune_result {
@@ -249,6 +251,40 @@ int xk_beam_to_rays(xk_ctx* ctx, const xk_beam* beam, size_t n_beam, const doubl
 int xk_diffraction_beam(xk_ctx* ctx, const xk_beam* beam, size_t n_beam, const double* normals,
                         const size_t* good, size_t n_good, const xk_wave_params* params,
                         xk_field* out, int path, xk_stats* stats);
+
+/* ---- 2-D Fresnel propagation ---------------------------------------------
+ *
+ * waves::fresnel::fresnel_propagate (src/waves/fresnel.rs:53-106): rays at
+ * (x_j, z_j) on the source plane with complex amplitude es_j, screen of
+ * nx x nz points x_i = x_min + (x_max - x_min) * i / max(nx - 1, 1) (same in
+ * z) at distance `dist`, k = energy / CHBAR * 1e7,
+ *   U(x, z) = sum_j es_j exp(i k/(2 dist) ((x - x_j)^2 + (z - z_j)^2)),
+ * output index iz * nx + ix (z outer, as the reference).
+ *
+ * Paths:
+ *   XK_PATH_F64        the reference's sum in FP64, term for term (parity).
+ *   XK_PATH_SEPARABLE  the Fresnel kernel factorises over a regular screen,
+ *                      exp(i a r^2) = exp(i a dx^2) exp(i a dz^2), so the
+ *                      screen is one complex matrix product over the rays:
+ *                      FP64 phasors split into f16 hi + lo parts, multiplied
+ *                      on the tensor cores with f32 accumulation (three
+ *                      partial products), K-split and ray-chunk partials
+ *                      added in FP64. */
+typedef struct xk_fresnel_screen {
+    double x_min, x_max;
+    size_t nx;
+    double z_min, z_max;
+    size_t nz;
+} xk_fresnel_screen;
+
+/* Host buffers: rays (n_rays each), amp_re / amp_im (nx * nz each), and
+ * optionally x_pixels (nx) and z_pixels (nz), the FresnelResult coordinates
+ * (NULL to skip). nx * nz == 0 is a no-op; no rays give zeros. */
+int xk_fresnel_propagate(xk_ctx* ctx, const double* ray_x, const double* ray_z,
+                         const double* es_re, const double* es_im, size_t n_rays, double energy,
+                         double dist, const xk_fresnel_screen* screen, double* amp_re,
+                         double* amp_im, double* x_pixels, double* z_pixels, int path,
+                         xk_stats* stats);
 
 /* ---- batches of solves ------------------------------------------------------
  *

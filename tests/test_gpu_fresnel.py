@@ -1,0 +1,128 @@
+"""2-D Fresnel propagation on the device (xk_fresnel_propagate).
+
+XK_PATH_F64 is the reference's FP64 sum term for term and must match the
+oracle's restatement of src/waves/fresnel.rs:53-106 to 1e-10; the
+tensor-core separable product (XK_PATH_SEPARABLE) must match it to 1e-4
+(relative L2 over the complex screen). Screen coordinates are exact."""
+import numpy as np
+import pytest
+
+import xrt_rs
+from xrt_rs import FresnelScreen
+
+pytestmark = pytest.mark.gpu
+
+F64_TOL = 1e-10
+SEP_TOL = 1e-4
+
+
+def rays(n, seed, spread=0.05):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(0, spread, n)
+    z = rng.normal(0, spread, n)
+    es = rng.uniform(0.2, 1.0, n) * np.exp(1j * rng.uniform(-np.pi, np.pi, n))
+    return x, z, es
+
+
+def oracle_field(oracle, x, z, es, energy, dist, sc):
+    re, im = oracle.fresnel(x, z, es.real, es.imag, energy, dist, sc.x_min, sc.x_max, sc.nx,
+                            sc.z_min, sc.z_max, sc.nz)
+    return re + 1j * im
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def coords(lo, hi, n):
+    return lo + (hi - lo) * np.arange(n, dtype=np.float64) / float(max(n - 1, 1))
+
+
+CASES = [  # (n rays, screen, energy, dist)
+    (3001, FresnelScreen(-0.3, 0.3, 37, -0.2, 0.25, 29), 10000.0, 1000.0),
+    (777, FresnelScreen(-0.5, 0.5, 129, -0.5, 0.5, 129), 30000.0, 100.0),
+    (64, FresnelScreen(-0.1, 0.1, 300, 0.0, 0.0, 1), 8000.0, 5000.0),
+    (5000, FresnelScreen(0.2, 0.2, 1, -0.4, 0.4, 211), 1000.0, 20000.0),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_f64_matches_oracle(ctx, oracle, case):
+    n, sc, energy, dist = CASES[case]
+    x, z, es = rays(n, seed=case)
+    res = xrt_rs.fresnel_propagate(x, z, es, energy, dist, sc, path="f64", ctx=ctx)
+    ref = oracle_field(oracle, x, z, es, energy, dist, sc)
+    assert res.amplitude.shape == (sc.nx * sc.nz,)
+    assert rel(res.amplitude, ref) < F64_TOL
+    assert np.array_equal(res.x_pixels, coords(sc.x_min, sc.x_max, sc.nx))
+    assert np.array_equal(res.z_pixels, coords(sc.z_min, sc.z_max, sc.nz))
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_separable_matches_oracle(ctx, oracle, case):
+    n, sc, energy, dist = CASES[case]
+    x, z, es = rays(n, seed=case)
+    res, st = xrt_rs.fresnel_propagate(x, z, es, energy, dist, sc, ctx=ctx, return_stats=True)
+    ref = oracle_field(oracle, x, z, es, energy, dist, sc)
+    err = rel(res.amplitude, ref)
+    print(f"case {case}: separable rel L2 {err:.2e}, chunks {st['n_chunks']}, "
+          f"tiles {st['n_tiles']} x splits {st['groups']}")
+    assert st["path"] == xrt_rs._lib.XK_PATH_SEPARABLE
+    assert err < SEP_TOL
+    assert np.array_equal(res.x_pixels, coords(sc.x_min, sc.x_max, sc.nx))
+
+
+def test_separable_over_several_ray_chunks(ctx, oracle):
+    x, z, es = rays(2500, seed=9)
+    sc = FresnelScreen(-0.2, 0.2, 45, -0.2, 0.2, 33)
+    ctx.set_option("fresnel_chunk_rays", 512)
+    try:
+        res, st = xrt_rs.fresnel_propagate(x, z, es, 12000.0, 800.0, sc, ctx=ctx,
+                                           return_stats=True)
+    finally:
+        ctx.set_option("fresnel_chunk_rays", 0)
+    assert st["n_chunks"] == 5
+    assert rel(res.amplitude, oracle_field(oracle, x, z, es, 12000.0, 800.0, sc)) < SEP_TOL
+
+
+@pytest.mark.parametrize("path", ["f64", "separable"])
+def test_single_point_source(ctx, path):
+    """src/waves/fresnel.rs:127-145."""
+    res = xrt_rs.fresnel_propagate([0.0], [0.0], [1.0 + 0j], 10000.0, 1000.0,
+                                   FresnelScreen(-0.1, 0.1, 21, -0.1, 0.1, 21), path=path, ctx=ctx)
+    assert len(res.amplitude) == 21 * 21
+    a = np.abs(res.amplitude)
+    assert a[10 * 21 + 10] >= a[0] - 1e-6
+    assert np.allclose(a, 1.0, atol=1e-5)
+
+
+@pytest.mark.parametrize("path", ["f64", "separable"])
+def test_two_slit(ctx, path):
+    """src/waves/fresnel.rs:147-165."""
+    res = xrt_rs.fresnel_propagate([-0.01, 0.01], [0.0, 0.0], [1.0 + 0j, 1.0 + 0j], 10000.0,
+                                   1000.0, FresnelScreen(-0.1, 0.1, 101, 0.0, 0.0, 1), path=path,
+                                   ctx=ctx)
+    inten = res.intensity()
+    assert inten[50] > 0.0 and inten[60] > 0.0
+
+
+@pytest.mark.parametrize("path", ["f64", "separable"])
+def test_no_rays_and_zero_amplitudes(ctx, path):
+    sc = FresnelScreen(-0.1, 0.1, 5, -0.1, 0.1, 4)
+    res = xrt_rs.fresnel_propagate([], [], [], 10000.0, 1000.0, sc, path=path, ctx=ctx)
+    assert np.all(res.amplitude == 0)
+    res = xrt_rs.fresnel_propagate([0.0, 0.1], [0.0, 0.0], [0j, 0j], 10000.0, 1000.0, sc,
+                                   path=path, ctx=ctx)
+    assert np.all(res.amplitude == 0)
+
+
+def test_empty_screen_and_bad_arguments(ctx):
+    res = xrt_rs.fresnel_propagate([0.0], [0.0], [1 + 0j], 1e4, 1e3,
+                                   FresnelScreen(-1, 1, 0, -1, 1, 5), ctx=ctx)
+    assert res.amplitude.size == 0
+    with pytest.raises(ValueError):
+        xrt_rs.fresnel_propagate([0.0, 1.0], [0.0], [1 + 0j], 1e4, 1e3,
+                                 FresnelScreen(-1, 1, 2, -1, 1, 2), ctx=ctx)
+    with pytest.raises(ValueError):
+        xrt_rs.fresnel_propagate([0.0], [0.0], [1 + 0j], 1e4, 1e3,
+                                 FresnelScreen(-1, 1, 2, -1, 1, 2), path="f32", ctx=ctx)

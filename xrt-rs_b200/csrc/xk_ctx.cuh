@@ -20,4 +20,5 @@ struct xk_ctx {
     xk::PrOptions pr_opts;
     xk::DevBuf in_rays, in_pix, out_field;
     xk::DevBuf in_beam;  // beam columns, normals and good indices (xk_beam_* calls)
+    xk::FresnelWorkspace fresnel;
 };

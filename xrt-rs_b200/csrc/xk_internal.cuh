@@ -23,6 +23,9 @@ struct Status {
     bool ok() const { return code == XK_OK; }
     static Status Ok() { return Status{}; }
     static Status Err(int c, std::string m) { return Status{c, std::move(m)}; }
+    static Status FromCuda(cudaError_t e) {
+        return e == cudaSuccess ? Ok() : Err(XK_ERR_CUDA, cudaGetErrorString(e));
+    }
 };
 
 #define XK_CUDA_TRY(expr)                                                                  \
@@ -123,5 +126,46 @@ Status wave_enqueue(const WaveGrid& g, double* x, double* y, double* z, cudaStre
 // ep_re, ep_im, energy).
 Status beam_rays_enqueue(const BeamDev& beam, const uint64_t* good, size_t n_good,
                          double* const out[12], cudaStream_t stream);
+
+// ---- 2-D Fresnel propagation (xk_fresnel.cu) ------------------------------
+
+struct FresnelIn {
+    const double *rx, *rz, *er, *ei;  // device, n each
+    size_t n;
+    double energy, dist;
+    double x_min, x_max, z_min, z_max;
+    size_t nx, nz;
+    double max_amp;                   // max_j |es_j| (scales the f16 factors)
+    double *out_re, *out_im;          // device, nx * nz each
+};
+
+struct FresnelShape {
+    size_t m_pad = 0, n_pad = 0;  // padded rows of the A (screen z) and B (2 x screen x) factors
+    size_t kc = 0, k3 = 0;        // rays per chunk, f16 columns per factor row (6 kc)
+    size_t chunks = 0, tiles = 0;
+    int kb_total = 0, splits = 1; // 64-wide K blocks per chunk, K splits per output tile
+};
+
+struct FresnelWorkspace {
+    DevBuf coords, factors, partial, ctrl;
+    size_t factor_budget = size_t(2) << 30;  // bytes of f16 factors per ray chunk
+    size_t max_chunk_rays = 0;               // cap on rays per chunk (0 = budget only)
+};
+
+struct FresnelReport {
+    int kernels = 0;
+    double gemm_ms = 0.0;                       // device time of the tensor-core products
+    cudaEvent_t ev_gemm[2] = {nullptr, nullptr};  // set to time the products (synchronises per chunk)
+    FresnelShape shape;
+    int* d_err = nullptr;                       // device error word of the products
+};
+
+FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms, size_t factor_budget,
+                           size_t max_chunk_rays);
+
+// Enqueues screen coordinates into ws.coords (nx then nz doubles; the caller
+// sizes it) and the sum for `path` (XK_PATH_F64 or XK_PATH_SEPARABLE).
+Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t stream,
+                       int num_sms, int path, FresnelReport* rep);
 
 }  // namespace xk

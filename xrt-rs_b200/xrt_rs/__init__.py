@@ -28,6 +28,7 @@ __all__ = [
     "GpuContext", "kirchhoff_gpu", "kirchhoff_auto", "GPU_RAY_DTYPE", "GPU_PIXEL_DTYPE",
     "XkError", "XK_PATH_F64", "XK_PATH_F32PR", "RAY_FIELDS", "PIXEL_FIELDS", "Batch",
     "autotune", "WaveParams", "prepare_wave", "beam_to_diffraction_rays", "diffraction_from_beam",
+    "FresnelScreen", "FresnelResult", "fresnel_propagate",
 ]
 
 RAY_FIELDS = ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re", "ep_im", "energy")
@@ -363,3 +364,4 @@ def kirchhoff_auto(rays, pixels):
 
 from .waves import (WaveParams, prepare_wave, beam_to_diffraction_rays,  # noqa: E402
                     diffraction_from_beam)
+from .fresnel import FresnelScreen, FresnelResult, fresnel_propagate  # noqa: E402

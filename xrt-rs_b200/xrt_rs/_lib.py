@@ -25,6 +25,7 @@ XK_ERR_SHUTDOWN = 9
 
 XK_PATH_F64 = 0
 XK_PATH_F32PR = 1
+XK_PATH_SEPARABLE = 2
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -161,6 +162,11 @@ class XkPixelsOut(ctypes.Structure):
     _fields_ = XkPixels._fields_
 
 
+class XkFresnelScreen(ctypes.Structure):
+    _fields_ = [("x_min", ctypes.c_double), ("x_max", ctypes.c_double), ("nx", ctypes.c_size_t),
+                ("z_min", ctypes.c_double), ("z_max", ctypes.c_double), ("nz", ctypes.c_size_t)]
+
+
 # Every entry point include/xk.h declares, with its ctypes signature.
 _SIGNATURES = {
     "xk_init": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
@@ -215,6 +221,10 @@ _SIGNATURES = {
         ctypes.c_void_p, ctypes.POINTER(XkBeam), ctypes.c_size_t, _dp,
         ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t, ctypes.POINTER(XkWaveParams),
         ctypes.POINTER(XkField), ctypes.c_int, ctypes.POINTER(XkStats)]),
+    "xk_fresnel_propagate": (ctypes.c_int, [
+        ctypes.c_void_p, _dp, _dp, _dp, _dp, ctypes.c_size_t, ctypes.c_double, ctypes.c_double,
+        ctypes.POINTER(XkFresnelScreen), _dp, _dp, _dp, _dp, ctypes.c_int,
+        ctypes.POINTER(XkStats)]),
     "xk_kirchhoff_auto": (ctypes.c_int, [
         ctypes.POINTER(XkGpuRay), ctypes.c_size_t, ctypes.POINTER(XkGpuPixel), ctypes.c_size_t,
         _dp]),
