@@ -62,9 +62,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sweep", type=int, default=-1, help="-1 auto, 0 SFU reciprocal, 1 packed")
     ap.add_argument("--phase-budget", type=float, default=512.0)
-    ap.add_argument("--workload", choices=["single", "batch", "sweep", "serve"], default="single",
+    ap.add_argument("--workload", choices=["single", "batch", "sweep", "serve", "fresnel"],
+                    default="single",
                     help="single: the 2^20 x 512^2 solve (default); batch: 64 uneven solves; "
-                         "sweep: the energy x distance precision sweep")
+                         "sweep: the energy x distance precision sweep; serve: Poisson "
+                         "arrivals through the server; fresnel: 2-D Fresnel propagation")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate [1/s]")
     ap.add_argument("--duration", type=float, default=60.0, help="serve: arrival window [s]")
     ap.add_argument("--drain", type=float, default=60.0,
@@ -343,6 +345,92 @@ def run_sweep(args):
     return 0
 
 
+def run_fresnel(args):
+    """2-D Fresnel propagation (src/waves/fresnel.rs:53-106): the aperture's
+    2^20 rays (x, z) with complex amplitudes onto a 512x512 screen of
+    +-0.5 mm at 1000 mm, 10 keV. The separable tensor-core product against the
+    FP64 direct sum on the same inputs, the oracle on one screen row as the
+    CPU baseline; the product kernel against the measured bf16 tensor peak."""
+    import torch
+    import xrt_rs
+    from oracle import oracle
+    from xrt_rs import synth
+
+    torch.cuda.set_device(0)
+    ctx = xrt_rs.GpuContext.new(0)
+    rays, _ = synth.config1(seed=0, n_rays=args.rays, grid=8)
+    x, z = rays["x"], rays["y"]
+    es = rays["es_re"] + 1j * rays["es_im"]
+    g = args.grid
+    sc = xrt_rs.FresnelScreen(-0.5, 0.5, g, -0.5, 0.5, g)
+    energy, dist = 10000.0, 1000.0
+    pairs = float(len(x)) * g * g
+    for _ in range(args.warmup):
+        xrt_rs.fresnel_propagate(x, z, es, energy, dist, sc, ctx=ctx)
+    clocks = ClockSampler(0)
+    clocks.start()
+    dev_ms, wall_ms, gemm_ms = [], [], []
+    for _ in range(args.steps):
+        res, st = xrt_rs.fresnel_propagate(x, z, es, energy, dist, sc, ctx=ctx, return_stats=True)
+        dev_ms.append(st["gpu_ms"])
+        wall_ms.append(st["wall_ms"])
+        gemm_ms.append(st["main_kernel_ms"])
+    clk = clocks.stop()
+    ref64, st64 = xrt_rs.fresnel_propagate(x, z, es, energy, dist, sc, path="f64", ctx=ctx,
+                                           return_stats=True)
+    err = float(np.linalg.norm(res.amplitude - ref64.amplitude) / np.linalg.norm(ref64.amplitude))
+    # Tensor work: per pair one complex multiply-add (8 real flops) in each of
+    # the three f16 partial products.
+    algo_flops = 24.0 * pairs
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    gemm = float(np.mean(gemm_ms))
+    achieved = algo_flops / (gemm / 1e3) / 1e12
+    cpu = None
+    if not args.no_cpu:
+        row = xrt_rs.FresnelScreen(-0.5, 0.5, g, 0.0, 0.0, 1)
+        t0 = time.perf_counter()
+        oracle.fresnel(x, z, es.real, es.imag, energy, dist, row.x_min, row.x_max, g, 0.0, 0.0, 1)
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(x) * g / dt / 1e9, "unit": UNIT, "cores": oracle.max_threads(),
+               "kind": "port",
+               "sample": f"{len(x)} rays x one {g}-point screen row ({dt:.1f} s, C restatement "
+                         f"of src/waves/fresnel.rs:53-106, OpenMP over screen points)"}
+    dev = float(np.mean(dev_ms))
+    line = {
+        "workload": "fresnel", "metric": "Gpair/s (ray x screen pair evaluations)",
+        "value": pairs / (dev / 1e3) / 1e9, "unit": UNIT, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev, "dtype": "f16x3 products, f32/f64 accumulation",
+        "data": "synthetic",
+        "config": {"workload": f"fresnel: {len(x)} rays x {g}x{g} screen +-0.5 mm at 1000 mm, "
+                               "10 keV", "rays": len(x), "screen_points": g * g,
+                   "pairs_per_step": pairs, "chunks": st["n_chunks"],
+                   "tiles": st["n_tiles"], "k_splits": st["groups"]},
+        "e2e": {"value": pairs / (float(np.mean(wall_ms)) / 1e3) / 1e9, "unit": UNIT,
+                "ms_per_step": float(np.mean(wall_ms)), "h2d_bytes_per_step": st["h2d_bytes"],
+                "d2h_bytes_per_step": st["d2h_bytes"]},
+        "fp64_direct": {"value": pairs / (st64["gpu_ms"] / 1e3) / 1e9, "unit": UNIT,
+                        "ms_per_step": st64["gpu_ms"],
+                        "speedup_separable_vs_f64": st64["gpu_ms"] / dev,
+                        "rel_l2_separable_vs_f64": err},
+        "roofline": {"bound": "tensor", "kernel": "fresnel_gemm_kernel",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "kernel_ms": gemm,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst; f16 runs at the "
+                                    "bf16 rate)",
+                     "algorithmic_flops": algo_flops},
+        "cpu_baseline": cpu, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_serve(args):
     """Poisson request stream through the continuous-batching server.
 
@@ -470,6 +558,8 @@ def main():
         return run_sweep(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "fresnel":
+        return run_fresnel(args)
 
     import torch
     import xrt_rs

@@ -126,3 +126,18 @@ def test_empty_screen_and_bad_arguments(ctx):
     with pytest.raises(ValueError):
         xrt_rs.fresnel_propagate([0.0], [0.0], [1 + 0j], 1e4, 1e3,
                                  FresnelScreen(-1, 1, 2, -1, 1, 2), path="f32", ctx=ctx)
+
+
+def test_separable_long_accumulation_against_f64(ctx):
+    """Few K splits per output tile (a 1024x1024 screen has 64 tiles), so each
+    CTA accumulates ~900 K blocks: the segmented FP64 drain keeps the product
+    as accurate as in the short-K cases (checked against the GPU FP64 sum,
+    itself pinned to the oracle above)."""
+    x, z, es = rays(20_000, seed=11, spread=0.1)
+    sc = FresnelScreen(-0.5, 0.5, 1024, -0.5, 0.5, 1024)
+    sep, st = xrt_rs.fresnel_propagate(x, z, es, 10000.0, 1000.0, sc, ctx=ctx, return_stats=True)
+    ref = xrt_rs.fresnel_propagate(x, z, es, 10000.0, 1000.0, sc, path="f64", ctx=ctx)
+    err = rel(sep.amplitude, ref.amplitude)
+    print(f"long K: rel L2 {err:.2e}, tiles {st['n_tiles']} x splits {st['groups']}")
+    assert st["groups"] <= 4
+    assert err < 1e-5

@@ -27,12 +27,13 @@
 //   K range split across CTAs, and split and chunk partials are added in
 //   FP64 in a fixed order (results do not depend on scheduling).
 //
-// The GEMM kernel: one CTA per 128 x 256 output tile and K range, 128
+// The GEMM kernel: one CTA per 128 x 256 output tile and K range, 192
 // threads; thread 0 issues TMA loads of 128x64 (A) and 256x64 (B) f16 tiles
 // with the 128-byte swizzle into a 4-stage ring, thread 32 issues four
-// 128x256x16 UMMAs per stage and commits each stage back to the producer,
-// then all four warps read the accumulator out of tensor memory (one 32-lane
-// quarter each) and store it as an f32 split partial.
+// 128x256x16 UMMAs per stage and commits each stage back to the producer;
+// every kSeg stages the accumulator (one of two in tensor memory) is handed
+// to four epilogue warps, which read it out (one 32-lane quarter each) and
+// add it into the CTA's FP64 split partial while the next segment runs.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -114,7 +115,9 @@ constexpr int kBM = 128, kBN = 256, kBK = 64, kStages = 4;
 constexpr uint32_t kABytes = kBM * kBK * 2, kBBytes = kBN * kBK * 2;
 constexpr uint32_t kStageBytes = kABytes + kBBytes;
 constexpr size_t kGemmSmem = 1024 + (size_t)kStages * kStageBytes + 256;
-constexpr int kGemmThreads = 128;
+constexpr int kEpiThreads = 128;                 // four epilogue warps
+constexpr int kGemmThreads = 64 + kEpiThreads;   // producer warp, UMMA warp, epilogue
+constexpr int kSeg = 32;                         // K blocks per f32 accumulation segment
 
 // exp(i a (p - r)^2) with the phase formed in FP64 and reduced to turns.
 __device__ __forceinline__ void phasor(double p, double r, double a, double* c, double* s) {
@@ -179,10 +182,17 @@ __global__ void factor_b_kernel(const double* __restrict__ xp, size_t nx,
     r1[2 * kc + j] = __halves2half2(ih, rh);
 }
 
-// C partial[split][m][n] (f32) = A[m, K range] * B[n, K range]^T.
+// partial[split][m][n] (FP64) = A[m, K range] * B[n, K range]^T.
+//
+// The tensor cores accumulate in f32; over long K ranges their accumulation
+// error grows with the number of accumulated blocks, so the K range is
+// processed in segments of kSeg blocks, each into a fresh accumulator, and
+// every finished segment is drained into the FP64 partial. Two accumulators
+// (512 TMEM columns) alternate: the UMMA thread fills one while the four
+// epilogue warps drain the other.
 __global__ void __launch_bounds__(kGemmThreads, 1)
 fresnel_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                    int kb_total, int splits, float* __restrict__ partial, int m_pad, int n_pad,
+                    int kb_total, int splits, double* __restrict__ partial, int m_pad, int n_pad,
                     int* __restrict__ err) {
     using namespace sm100;
     extern __shared__ unsigned char smem_raw[];
@@ -190,8 +200,9 @@ fresnel_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(tiles + kStages * kStageBytes);
     uint64_t* empty = full + kStages;
-    uint64_t* done = empty + kStages;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* acc_full = empty + kStages;
+    uint64_t* acc_empty = acc_full + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
     volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -199,26 +210,30 @@ fresnel_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
     const int kb0 = (int)((long long)kb_total * sp / splits);
     const int kb1 = (int)((long long)kb_total * (sp + 1) / splits);
     const int nkb = kb1 - kb0;
+    const int nseg = (nkb + kSeg - 1) / kSeg;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], kEpiThreads);
+        }
         mbar_init_fence();
         *flag = 0;
         prefetch_tensor_map(&tmA);
         prefetch_tensor_map(&tmB);
     }
-    if (warp == 1) tmem_alloc(tmem_slot, kBN);
+    if (warp == 1) tmem_alloc(tmem_slot, 2 * kBN);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
     if (threadIdx.x == 0) {
-        // TMA producer.
+        // TMA producer over the whole K range.
         for (int i = 0; i < nkb; ++i) {
             const int s = i % kStages;
             const uint32_t ph = (uint32_t)(i / kStages) & 1u;
@@ -233,58 +248,90 @@ fresnel_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             tma_load_2d(a + kABytes, &tmB, kx, nt * kBN, &full[s]);
         }
     } else if (threadIdx.x == 32) {
-        // UMMA issuer.
+        // UMMA issuer: segment g accumulates into buffer g & 1.
         constexpr uint32_t idesc = idesc_f16_f32(kBM, kBN);
-        for (int i = 0; i < nkb; ++i) {
-            const int s = i % kStages;
-            const uint32_t ph = (uint32_t)(i / kStages) & 1u;
-            if (!mbar_wait(&full[s], ph)) {
+        bool good = true;
+        for (int g = 0; g < nseg && good; ++g) {
+            const int b = g & 1, use = g >> 1;
+            if (use >= 1 && !mbar_wait(&acc_empty[b], (uint32_t)(use - 1) & 1u)) {
                 *flag = 1;
                 break;
             }
             tc_fence_after();
-            const uint32_t a = smem_u32(tiles + (size_t)s * kStageBytes);
-            const uint32_t b = a + kABytes;
+            const uint32_t d = tmem + (uint32_t)(b * kBN);
+            const int i0 = g * kSeg, i1 = min(nkb, i0 + kSeg);
+            for (int i = i0; i < i1; ++i) {
+                const int s = i % kStages;
+                const uint32_t ph = (uint32_t)(i / kStages) & 1u;
+                if (!mbar_wait(&full[s], ph)) {
+                    *flag = 1;
+                    good = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a = smem_u32(tiles + (size_t)s * kStageBytes);
+                const uint32_t bb = a + kABytes;
 #pragma unroll
-            for (int k = 0; k < kBK / 16; ++k)
-                umma_f16(tmem, desc_kmajor_sw128(a + 32u * k), desc_kmajor_sw128(b + 32u * k),
-                         idesc, (uint32_t)(i | k));
-            umma_commit(&empty[s]);
+                for (int k = 0; k < kBK / 16; ++k)
+                    umma_f16(d, desc_kmajor_sw128(a + 32u * k), desc_kmajor_sw128(bb + 32u * k),
+                             idesc, (uint32_t)((i - i0) | k));
+                umma_commit(&empty[s]);
+            }
+            umma_commit(&acc_full[b]);  // arrives once the segment's UMMAs have completed
         }
-        umma_commit(done);  // arrives once every UMMA above has completed
+    } else if (warp >= 2) {
+        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its quarter).
+        const int q = warp & 3;
+        const int row = mt * kBM + q * 32 + lane;
+        double* dst = partial + ((size_t)sp * m_pad + row) * n_pad + (size_t)nt * kBN;
+        if (nseg == 0) {
+            for (int c = 0; c < kBN; c += 2)
+                *reinterpret_cast<double2*>(dst + c) = make_double2(0.0, 0.0);
+        }
+        for (int g = 0; g < nseg; ++g) {
+            const int b = g & 1;
+            const bool ok = mbar_wait(&acc_full[b], (uint32_t)(g >> 1) & 1u);
+            if (!__all_sync(0xffffffffu, ok)) {
+                *flag = 1;
+                break;
+            }
+            tc_fence_after();
+#pragma unroll 1
+            for (int c = 0; c < kBN / 32; ++c) {
+                float v[32];
+                tmem_ld_32cols(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kBN + c * 32), v);
+                double2* d2 = reinterpret_cast<double2*>(dst + c * 32);
+                if (g == 0) {
+#pragma unroll
+                    for (int t = 0; t < 16; ++t)
+                        d2[t] = make_double2((double)v[2 * t], (double)v[2 * t + 1]);
+                } else {
+#pragma unroll
+                    for (int t = 0; t < 16; ++t) {
+                        double2 o = d2[t];
+                        o.x += (double)v[2 * t];
+                        o.y += (double)v[2 * t + 1];
+                        d2[t] = o;
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&acc_empty[b]);
+        }
     }
     __syncthreads();
-    const bool ok = __syncthreads_and(mbar_wait(done, 0) && *flag == 0);
-    tc_fence_after();
-
-    const int row = mt * kBM + warp * 32 + lane;
-    float* dst = partial + ((size_t)sp * m_pad + row) * n_pad + (size_t)nt * kBN;
-    if (ok && nkb > 0) {
-#pragma unroll 1
-        for (int c = 0; c < kBN / 32; ++c) {
-            float v[32];
-            tmem_ld_32cols(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32), v);
-            float4* d4 = reinterpret_cast<float4*>(dst + c * 32);
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                d4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-        }
-    } else {
-        for (int c = 0; c < kBN; c += 4)
-            *reinterpret_cast<float4*>(dst + c) = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (!ok && threadIdx.x == 0) atomicExch(err, 1);
-    }
+    if (*flag != 0 && threadIdx.x == 0) atomicExch(err, 1);
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_free(tmem, kBN);
+        tmem_free(tmem, 2 * kBN);
     }
 }
 
 // acc[iz*nx + ix] (+)= scale * sum over splits of C[iz][2ix + c], in FP64 and
 // split order.
-__global__ void reduce_kernel(const float* __restrict__ partial, int splits, int m_pad, int n_pad,
+__global__ void reduce_kernel(const double* __restrict__ partial, int splits, int m_pad, int n_pad,
                               size_t nz, size_t nx, double scale, double* __restrict__ acc_re,
                               double* __restrict__ acc_im, int first) {
     const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -292,10 +339,10 @@ __global__ void reduce_kernel(const float* __restrict__ partial, int splits, int
     const size_t iz = idx / nx, ix = idx - iz * nx;
     double re = 0.0, im = 0.0;
     for (int s = 0; s < splits; ++s) {
-        const float2 v = *reinterpret_cast<const float2*>(
+        const double2 v = *reinterpret_cast<const double2*>(
             partial + ((size_t)s * m_pad + iz) * n_pad + 2 * ix);
-        re += (double)v.x;
-        im += (double)v.y;
+        re += v.x;
+        im += v.y;
     }
     re *= scale;
     im *= scale;
@@ -390,7 +437,7 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     }
     const FresnelShape sh = fresnel_shape(n, nx, nz, num_sms, ws.factor_budget, ws.max_chunk_rays);
     XK_TRY(ws.factors.ensure((sh.m_pad + sh.n_pad) * sh.k3 * sizeof(__half)));
-    XK_TRY(ws.partial.ensure((size_t)sh.splits * sh.m_pad * sh.n_pad * sizeof(float)));
+    XK_TRY(ws.partial.ensure((size_t)sh.splits * sh.m_pad * sh.n_pad * sizeof(double)));
     XK_TRY(ws.ctrl.ensure(256));
     __half* A = ws.factors.as<__half>();
     __half* B = A + sh.m_pad * sh.k3;
@@ -421,7 +468,7 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
         const bool timed = rep->ev_gemm[0] && rep->ev_gemm[1];
         if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[0], stream));
         fresnel_gemm_kernel<<<grid, kGemmThreads, kGemmSmem, stream>>>(
-            mapA, mapB, sh.kb_total, sh.splits, ws.partial.as<float>(), (int)sh.m_pad,
+            mapA, mapB, sh.kb_total, sh.splits, ws.partial.as<double>(), (int)sh.m_pad,
             (int)sh.n_pad, d_err);
         XK_CUDA_TRY(cudaGetLastError());
         if (timed) {
@@ -431,7 +478,7 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
             XK_CUDA_TRY(cudaEventElapsedTime(&ms, rep->ev_gemm[0], rep->ev_gemm[1]));
             rep->gemm_ms += ms;
         }
-        reduce_kernel<<<grid_1d(m, 256), 256, 0, stream>>>(ws.partial.as<float>(), sh.splits,
+        reduce_kernel<<<grid_1d(m, 256), 256, 0, stream>>>(ws.partial.as<double>(), sh.splits,
                                                             (int)sh.m_pad, (int)sh.n_pad, nz, nx,
                                                             in.max_amp, in.out_re, in.out_im,
                                                             c == 0);
