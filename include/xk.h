@@ -144,9 +144,7 @@ const char* xk_route_reason(int reason);
  *   "phase_budget"   bound on the FP32 residual phase in rad (default 512)
  *   "sweep"          -1 automatic, 0 SFU reciprocal, 1 packed f32x2 sweep
  *   "groups"         ray ranges per screen tile, 0 = automatic
- *   "items_per_warp" target work items per resident warp (automatic groups)
- *   "fresnel_chunk_rays" cap on rays per chunk of the separable Fresnel
- *                    product (0 = sized by its 2 GiB factor budget) */
+ *   "items_per_warp" target work items per resident warp (automatic groups) */
 int xk_set_option(xk_ctx* ctx, const char* name, double value);
 
 typedef struct xk_tune_result {
@@ -266,10 +264,11 @@ int xk_diffraction_beam(xk_ctx* ctx, const xk_beam* beam, size_t n_beam, const d
  *   XK_PATH_SEPARABLE  the Fresnel kernel factorises over a regular screen,
  *                      exp(i a r^2) = exp(i a dx^2) exp(i a dz^2), so the
  *                      screen is one complex matrix product over the rays:
- *                      FP64 phasors split into f16 hi + lo parts, multiplied
- *                      on the tensor cores with f32 accumulation (three
- *                      partial products), K-split and ray-chunk partials
- *                      added in FP64. */
+ *                      phasors from FP64 phases, split into f16 hi + lo
+ *                      parts inside the kernel, multiplied on the tensor
+ *                      cores with f32 accumulation (three partial products),
+ *                      drained into FP64 every few ray blocks; K-split
+ *                      partials added in FP64. */
 typedef struct xk_fresnel_screen {
     double x_min, x_max;
     size_t nx;

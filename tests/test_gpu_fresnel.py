@@ -72,16 +72,14 @@ def test_separable_matches_oracle(ctx, oracle, case):
     assert np.array_equal(res.x_pixels, coords(sc.x_min, sc.x_max, sc.nx))
 
 
-def test_separable_over_several_ray_chunks(ctx, oracle):
-    x, z, es = rays(2500, seed=9)
+def test_separable_many_segments_and_splits(ctx, oracle):
+    """20011 rays on one output tile: K split over many CTAs, each running
+    several accumulation segments through both tensor-memory accumulators."""
+    x, z, es = rays(20011, seed=9)
     sc = FresnelScreen(-0.2, 0.2, 45, -0.2, 0.2, 33)
-    ctx.set_option("fresnel_chunk_rays", 512)
-    try:
-        res, st = xrt_rs.fresnel_propagate(x, z, es, 12000.0, 800.0, sc, ctx=ctx,
-                                           return_stats=True)
-    finally:
-        ctx.set_option("fresnel_chunk_rays", 0)
-    assert st["n_chunks"] == 5
+    res, st = xrt_rs.fresnel_propagate(x, z, es, 12000.0, 800.0, sc, ctx=ctx, return_stats=True)
+    assert st["n_tiles"] == 1 and st["groups"] >= 8
+    assert st["n_chunks"] == (20011 + 31) // 32  # ray blocks
     assert rel(res.amplitude, oracle_field(oracle, x, z, es, 12000.0, 800.0, sc)) < SEP_TOL
 
 

@@ -66,7 +66,6 @@ void destroy_ctx(xk_ctx* ctx) {
     ctx->out_field.release();
     ctx->in_beam.release();
     ctx->fresnel.coords.release();
-    ctx->fresnel.factors.release();
     ctx->fresnel.partial.release();
     ctx->fresnel.ctrl.release();
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -310,11 +309,6 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
     if (!ctx || !name) return XK_ERR_INVALID;
     std::lock_guard<std::mutex> lock(ctx->mu);
     std::string n(name);
-    if (n == "fresnel_chunk_rays") {
-        if (!(value >= 0.0) || value > 1e9) return fail(ctx, XK_ERR_INVALID, "fresnel_chunk_rays out of range");
-        ctx->fresnel.max_chunk_rays = (size_t)value;
-        return XK_OK;
-    }
     if (n == "phase_budget") {
         if (!(value > 0.0) || value > 1e5) return fail(ctx, XK_ERR_INVALID, "phase_budget out of range");
         ctx->pr_opts.phase_budget = value;

@@ -19,21 +19,18 @@
 //       C[iz][2 ix + c] = sum_k A[iz][k] B[2 ix + c][k],
 //       A[iz][2j] = Re Z, A[iz][2j+1] = Im Z,
 //       B[2ix][2j] = Re W, B[2ix][2j+1] = -Im W, B[2ix+1][2j] = Im W, B[2ix+1][2j+1] = Re W,
-//   with W = es X / max|es|. The factors (unit phasors, phases in FP64) are
-//   written in f16 as hi + lo pairs and multiplied on the tensor cores
-//   (tcgen05.mma kind::f16, f32 accumulators in tensor memory) as
-//   A_hi B_hi + A_hi B_lo + A_lo B_hi (three K-blocks of one product), which
-//   keeps ~2^-22 of each phasor; rays are processed in chunks, each chunk's
-//   K range split across CTAs, and split and chunk partials are added in
-//   FP64 in a fixed order (results do not depend on scheduling).
-//
-// The GEMM kernel: one CTA per 128 x 256 output tile and K range, 192
-// threads; thread 0 issues TMA loads of 128x64 (A) and 256x64 (B) f16 tiles
-// with the 128-byte swizzle into a 4-stage ring, thread 32 issues four
-// 128x256x16 UMMAs per stage and commits each stage back to the producer;
-// every kSeg stages the accumulator (one of two in tensor memory) is handed
-// to four epilogue warps, which read it out (one 32-lane quarter each) and
-// add it into the CTA's FP64 split partial while the next segment runs.
+//   with W = es X / max|es|. One fused kernel computes it on the tensor
+//   cores without ever writing A or B to memory: per block of 32 rays, eight
+//   producer warps form the CTA's A (128 z rows) and B (128 x points, 256
+//   rows) tiles from FP64 phases, split each phasor into f16 hi + lo parts
+//   and store them in shared memory in the 128-byte-swizzled K-major layout;
+//   one thread issues tcgen05.mma kind::f16 (f32 accumulation in tensor
+//   memory) for A_hi B_hi + A_hi B_lo + A_lo B_hi, which keeps ~2^-21 of each
+//   phasor; four epilogue warps drain the accumulator into an FP64 partial
+//   every kFSeg ray blocks (the tensor cores' f32 accumulation error grows
+//   with the number of accumulated blocks), alternating between two TMEM
+//   accumulators so that draining overlaps the next segment. K-split partials
+//   are added in FP64 in split order (results do not depend on scheduling).
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -109,199 +106,164 @@ fresnel_f64_kernel(const double* __restrict__ rx, const double* __restrict__ rz,
     }
 }
 
-// ---- separable product on the tensor cores -----------------------------------
+// ---- fused separable product on the tensor cores --------------------------------
 
-constexpr int kBM = 128, kBN = 256, kBK = 64, kStages = 4;
-constexpr uint32_t kABytes = kBM * kBK * 2, kBBytes = kBN * kBK * 2;
-constexpr uint32_t kStageBytes = kABytes + kBBytes;
-constexpr size_t kGemmSmem = 1024 + (size_t)kStages * kStageBytes + 256;
-constexpr int kEpiThreads = 128;                 // four epilogue warps
-constexpr int kGemmThreads = 64 + kEpiThreads;   // producer warp, UMMA warp, epilogue
-constexpr int kSeg = 32;                         // K blocks per f32 accumulation segment
+constexpr int kFRays = 32;                       // rays per block: K = 64 halves (re, im)
+constexpr int kFStages = 2;
+constexpr uint32_t kFA = 128 * 64 * 2;           // one A tile (hi or lo): 128 rows x 128 B
+constexpr uint32_t kFB = 256 * 64 * 2;           // one B tile: 256 rows x 128 B
+constexpr uint32_t kFStage = 2 * kFA + 2 * kFB;  // A_hi | A_lo | B_hi | B_lo
+constexpr int kFEpiThreads = 128;                // warps 1..4
+constexpr int kFProdThreads = 256;               // warps 5..12
+constexpr int kFThreads = 32 + kFEpiThreads + kFProdThreads;
+constexpr int kFSeg = 20;                        // ray blocks (60 K blocks) per f32 segment
+constexpr int kFN = 256;                         // accumulator columns (N of the UMMA)
+// Ray staging (two blocks): rx, rz (f64) and the scaled amplitude (f32 x 2).
+constexpr uint32_t kFRayBytes = kFRays * (8 + 8 + 8);
+constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + 2 * kFRayBytes + 256;
 
-// exp(i a (p - r)^2) with the phase formed in FP64 and reduced to turns.
-__device__ __forceinline__ void phasor(double p, double r, double a, double* c, double* s) {
+struct FusedArgs {
+    const double *rx, *rz, *er, *ei;
+    size_t n;
+    int ray_blocks, splits;
+    const double *xp, *zp;
+    size_t nx, nz;
+    double a_turns;    // k / (2 d) / (2 pi)
+    double inv_scale;  // 1 / max|es|
+    double* partial;   // [splits][m_pad][n_pad]
+    int m_pad, n_pad;
+    int* err;
+};
+
+// Byte offset of 16-byte chunk c (0..7) of row r in a 128-byte-swizzled tile.
+__device__ __forceinline__ uint32_t sw128(uint32_t r, uint32_t c) {
+    return r * 128u + ((c ^ (r & 7u)) << 4);
+}
+
+// exp(2 pi i t), t = a_turns (p - r)^2 in turns, reduced in FP64.
+__device__ __forceinline__ void phasor_t(double p, double r, double a_turns, float* c, float* s) {
     const double d = p - r;
-    const double turns = a * d * d * kInv2Pi;
-    const double f = turns - rint(turns);
-    sincospi(2.0 * f, s, c);
+    const double t = (a_turns * d) * d;
+    const float f = (float)(t - rint(t));
+    __sincosf(6.28318530717958647692f * f, s, c);
 }
 
-__device__ __forceinline__ void split_h(double v, __half* hi, __half* lo) {
-    *hi = __double2half(v);
-    *lo = __double2half(v - (double)__half2float(*hi));
+// (a, b) -> f16x2 hi (round to nearest) and f16x2 lo = (a, b) - hi.
+__device__ __forceinline__ void split16x2(float a, float b, uint32_t* hi, uint32_t* lo) {
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 back = __half22float2(h);
+    const __half2 l = __floats2half2_rn(a - back.x, b - back.y);
+    *hi = *reinterpret_cast<const uint32_t*>(&h);
+    *lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
-// A rows (screen z): row iz of K3 = 6 kc halves, ray j of the chunk at
-// columns 2j (re), 2j+1 (im) of each of the three K blocks [hi | hi | lo].
-__global__ void factor_a_kernel(const double* __restrict__ zp, size_t nz,
-                                const double* __restrict__ rz, size_t n, size_t j0, size_t kc,
-                                double a, __half* __restrict__ A, size_t K3) {
-    const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (idx >= nz * kc) return;
-    const size_t iz = idx / kc, j = idx - iz * kc, jj = j0 + j;
-    double c = 0.0, s = 0.0;
-    if (jj < n) phasor(zp[iz], rz[jj], a, &c, &s);
-    __half ch, cl, sh, sl;
-    split_h(c, &ch, &cl);
-    split_h(s, &sh, &sl);
-    __half2* row = reinterpret_cast<__half2*>(A + iz * K3);
-    row[j] = __halves2half2(ch, sh);
-    row[kc + j] = __halves2half2(ch, sh);
-    row[2 * kc + j] = __halves2half2(cl, sl);
+// (x, y) -> (x, -y) and (y, x) on packed f16 pairs (sign flip, half swap).
+__device__ __forceinline__ uint32_t neg_hi(uint32_t v) { return v ^ 0x80000000u; }
+__device__ __forceinline__ uint32_t swap_halves(uint32_t v) { return __byte_perm(v, 0, 0x1032); }
+
+__device__ __forceinline__ void producer_sync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(kFProdThreads) : "memory");
 }
 
-// B rows (screen x, two per point): [hi | lo | hi] blocks of the W matrix.
-__global__ void factor_b_kernel(const double* __restrict__ xp, size_t nx,
-                                const double* __restrict__ rx, const double* __restrict__ er,
-                                const double* __restrict__ ei, size_t n, size_t j0, size_t kc,
-                                double a, double inv_scale, __half* __restrict__ B, size_t K3) {
-    const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (idx >= nx * kc) return;
-    const size_t ix = idx / kc, j = idx - ix * kc, jj = j0 + j;
-    double wr = 0.0, wi = 0.0;
-    if (jj < n) {
-        double c, s;
-        phasor(xp[ix], rx[jj], a, &c, &s);
-        const double e_r = er[jj] * inv_scale, e_i = ei[jj] * inv_scale;
-        wr = e_r * c - e_i * s;
-        wi = e_r * s + e_i * c;
-    }
-    __half rh, rl, ih, il, nih, nil;
-    split_h(wr, &rh, &rl);
-    split_h(wi, &ih, &il);
-    nih = __hneg(ih);
-    nil = __hneg(il);
-    __half2* r0 = reinterpret_cast<__half2*>(B + (2 * ix) * K3);
-    __half2* r1 = reinterpret_cast<__half2*>(B + (2 * ix + 1) * K3);
-    r0[j] = __halves2half2(rh, nih);
-    r0[kc + j] = __halves2half2(rl, nil);
-    r0[2 * kc + j] = __halves2half2(rh, nih);
-    r1[j] = __halves2half2(ih, rh);
-    r1[kc + j] = __halves2half2(il, rl);
-    r1[2 * kc + j] = __halves2half2(ih, rh);
-}
-
-// partial[split][m][n] (FP64) = A[m, K range] * B[n, K range]^T.
-//
-// The tensor cores accumulate in f32; over long K ranges their accumulation
-// error grows with the number of accumulated blocks, so the K range is
-// processed in segments of kSeg blocks, each into a fresh accumulator, and
-// every finished segment is drained into the FP64 partial. Two accumulators
-// (512 TMEM columns) alternate: the UMMA thread fills one while the four
-// epilogue warps drain the other.
-__global__ void __launch_bounds__(kGemmThreads, 1)
-fresnel_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                    int kb_total, int splits, double* __restrict__ partial, int m_pad, int n_pad,
-                    int* __restrict__ err) {
+__global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g) {
     using namespace sm100;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* tiles = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-    uint64_t* full = reinterpret_cast<uint64_t*>(tiles + kStages * kStageBytes);
-    uint64_t* empty = full + kStages;
-    uint64_t* acc_full = empty + kStages;
+    uint64_t* full = reinterpret_cast<uint64_t*>(tiles + kFStages * kFStage);
+    uint64_t* empty = full + kFStages;
+    uint64_t* acc_full = empty + kFStages;
     uint64_t* acc_empty = acc_full + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
     volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    unsigned char* rays_smem = reinterpret_cast<unsigned char*>(tmem_slot) + 64;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = blockIdx.x, nt = blockIdx.y, sp = blockIdx.z;
-    const int kb0 = (int)((long long)kb_total * sp / splits);
-    const int kb1 = (int)((long long)kb_total * (sp + 1) / splits);
-    const int nkb = kb1 - kb0;
-    const int nseg = (nkb + kSeg - 1) / kSeg;
+    const int rb0 = (int)((long long)g.ray_blocks * sp / g.splits);
+    const int rb1 = (int)((long long)g.ray_blocks * (sp + 1) / g.splits);
+    const int nrb = rb1 - rb0;
+    const int nseg = (nrb + kFSeg - 1) / kFSeg;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            mbar_init(&full[s], 1);
+        for (int s = 0; s < kFStages; ++s) {
+            mbar_init(&full[s], kFProdThreads / 32);  // one arrival per producer warp
             mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], kEpiThreads);
+            mbar_init(&acc_empty[b], kFEpiThreads);
         }
         mbar_init_fence();
         *flag = 0;
-        prefetch_tensor_map(&tmA);
-        prefetch_tensor_map(&tmB);
     }
-    if (warp == 1) tmem_alloc(tmem_slot, 2 * kBN);
+    if (warp == 0) tmem_alloc(tmem_slot, 2 * kFN);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (threadIdx.x == 0) {
-        // TMA producer over the whole K range.
-        for (int i = 0; i < nkb; ++i) {
-            const int s = i % kStages;
-            const uint32_t ph = (uint32_t)(i / kStages) & 1u;
-            if (!mbar_wait(&empty[s], ph ^ 1u)) {
-                *flag = 1;
-                break;
-            }
-            mbar_arrive_expect_tx(&full[s], kStageBytes);
-            unsigned char* a = tiles + (size_t)s * kStageBytes;
-            const int kx = (kb0 + i) * kBK;
-            tma_load_2d(a, &tmA, kx, mt * kBM, &full[s]);
-            tma_load_2d(a + kABytes, &tmB, kx, nt * kBN, &full[s]);
-        }
-    } else if (threadIdx.x == 32) {
-        // UMMA issuer: segment g accumulates into buffer g & 1.
-        constexpr uint32_t idesc = idesc_f16_f32(kBM, kBN);
-        bool good = true;
-        for (int g = 0; g < nseg && good; ++g) {
-            const int b = g & 1, use = g >> 1;
-            if (use >= 1 && !mbar_wait(&acc_empty[b], (uint32_t)(use - 1) & 1u)) {
-                *flag = 1;
-                break;
-            }
-            tc_fence_after();
-            const uint32_t d = tmem + (uint32_t)(b * kBN);
-            const int i0 = g * kSeg, i1 = min(nkb, i0 + kSeg);
-            for (int i = i0; i < i1; ++i) {
-                const int s = i % kStages;
-                const uint32_t ph = (uint32_t)(i / kStages) & 1u;
-                if (!mbar_wait(&full[s], ph)) {
+    if (warp == 0) {
+        if (lane == 0) {
+            // UMMA issuer: per ray block three K blocks (hi.hi, hi.lo, lo.hi);
+            // segment q accumulates into buffer q & 1.
+            constexpr uint32_t idesc = idesc_f16_f32(128, kFN);
+            bool good = true;
+            for (int q = 0; q < nseg && good; ++q) {
+                const int b = q & 1, use = q >> 1;
+                if (use >= 1 && !mbar_wait(&acc_empty[b], (uint32_t)(use - 1) & 1u)) {
                     *flag = 1;
-                    good = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t a = smem_u32(tiles + (size_t)s * kStageBytes);
-                const uint32_t bb = a + kABytes;
+                const uint32_t d = tmem + (uint32_t)(b * kFN);
+                const int i0 = q * kFSeg, i1 = min(nrb, i0 + kFSeg);
+                for (int i = i0; i < i1; ++i) {
+                    const int s = i % kFStages;
+                    if (!mbar_wait(&full[s], (uint32_t)(i / kFStages) & 1u)) {
+                        *flag = 1;
+                        good = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_hi = smem_u32(tiles + (size_t)s * kFStage);
+                    const uint32_t a_lo = a_hi + kFA, b_hi = a_hi + 2 * kFA, b_lo = b_hi + kFB;
+                    const uint32_t as[3] = {a_hi, a_hi, a_lo}, bs[3] = {b_hi, b_lo, b_hi};
 #pragma unroll
-                for (int k = 0; k < kBK / 16; ++k)
-                    umma_f16(d, desc_kmajor_sw128(a + 32u * k), desc_kmajor_sw128(bb + 32u * k),
-                             idesc, (uint32_t)((i - i0) | k));
-                umma_commit(&empty[s]);
+                    for (int p = 0; p < 3; ++p)
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            umma_f16(d, desc_kmajor_sw128(as[p] + 32u * k),
+                                     desc_kmajor_sw128(bs[p] + 32u * k), idesc,
+                                     (uint32_t)((i - i0) | p | k));
+                    umma_commit(&empty[s]);
+                }
+                umma_commit(&acc_full[b]);
             }
-            umma_commit(&acc_full[b]);  // arrives once the segment's UMMAs have completed
         }
-    } else if (warp >= 2) {
-        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its quarter).
-        const int q = warp & 3;
-        const int row = mt * kBM + q * 32 + lane;
-        double* dst = partial + ((size_t)sp * m_pad + row) * n_pad + (size_t)nt * kBN;
-        if (nseg == 0) {
-            for (int c = 0; c < kBN; c += 2)
+        __syncwarp();
+    } else if (warp <= 4) {
+        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31.
+        const int qd = warp & 3;
+        const int row = mt * 128 + qd * 32 + lane;
+        double* dst = g.partial + ((size_t)sp * g.m_pad + row) * g.n_pad + (size_t)nt * kFN;
+        if (nseg == 0)
+            for (int c = 0; c < kFN; c += 2)
                 *reinterpret_cast<double2*>(dst + c) = make_double2(0.0, 0.0);
-        }
-        for (int g = 0; g < nseg; ++g) {
-            const int b = g & 1;
-            const bool ok = mbar_wait(&acc_full[b], (uint32_t)(g >> 1) & 1u);
+        for (int q = 0; q < nseg; ++q) {
+            const int b = q & 1;
+            const bool ok = mbar_wait(&acc_full[b], (uint32_t)(q >> 1) & 1u);
             if (!__all_sync(0xffffffffu, ok)) {
                 *flag = 1;
                 break;
             }
             tc_fence_after();
 #pragma unroll 1
-            for (int c = 0; c < kBN / 32; ++c) {
+            for (int c = 0; c < kFN / 32; ++c) {
                 float v[32];
-                tmem_ld_32cols(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kBN + c * 32), v);
+                tmem_ld_32cols(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * kFN + c * 32), v);
                 double2* d2 = reinterpret_cast<double2*>(dst + c * 32);
-                if (g == 0) {
+                if (q == 0) {
 #pragma unroll
                     for (int t = 0; t < 16; ++t)
                         d2[t] = make_double2((double)v[2 * t], (double)v[2 * t + 1]);
@@ -318,14 +280,108 @@ fresnel_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             tc_fence_before();
             mbar_arrive(&acc_empty[b]);
         }
+    } else {
+        // Producers: thread p owns A row r (screen z index mt*128 + r) and B
+        // rows 2r, 2r+1 (screen x index nt*128 + r) for rays 16h .. 16h+15 of
+        // each block (h = p / 128), i.e. 16-byte chunks 4h .. 4h+3 of its rows.
+        // The block's rays are staged in shared memory one block ahead by
+        // threads 0..95 (rx, rz, scaled amplitude).
+        const int p = threadIdx.x - 160;
+        const int h = p >> 7, r = p & 127;
+        const size_t iz = (size_t)mt * 128 + r, ix = (size_t)nt * 128 + r;
+        const bool va = iz < g.nz, vb = ix < g.nx;
+        const double zv = va ? g.zp[iz] : 0.0, xv = vb ? g.xp[ix] : 0.0;
+        auto stage_rx = [&](int buf) { return reinterpret_cast<double*>(rays_smem + buf * kFRayBytes); };
+        auto stage_rz = [&](int buf) { return stage_rx(buf) + kFRays; };
+        auto stage_e = [&](int buf) { return reinterpret_cast<float2*>(stage_rx(buf) + 2 * kFRays); };
+        // Value this thread stages for block `blk` (threads 0..95 only).
+        auto fetch = [&](int blk, double* dv, float2* ev) {
+            const size_t j = (size_t)(rb0 + blk) * kFRays + (p & 31);
+            const bool in = j < g.n;
+            if (p < 32) *dv = in ? __ldg(g.rx + j) : 0.0;
+            else if (p < 64) *dv = in ? __ldg(g.rz + j) : 0.0;
+            else if (p < 96)
+                *ev = in ? make_float2((float)(__ldg(g.er + j) * g.inv_scale),
+                                       (float)(__ldg(g.ei + j) * g.inv_scale))
+                         : make_float2(0.f, 0.f);
+        };
+        auto put = [&](int buf, double dv, float2 ev) {
+            if (p < 32) stage_rx(buf)[p] = dv;
+            else if (p < 64) stage_rz(buf)[p - 32] = dv;
+            else if (p < 96) stage_e(buf)[p - 64] = ev;
+        };
+        if (nrb > 0) {
+            double dv = 0.0;
+            float2 ev = make_float2(0.f, 0.f);
+            fetch(0, &dv, &ev);
+            put(0, dv, ev);
+        }
+        producer_sync();
+        for (int i = 0; i < nrb; ++i) {
+            const int s = i % kFStages, rbuf = i & 1;
+            double nd = 0.0;
+            float2 ne = make_float2(0.f, 0.f);
+            if (i + 1 < nrb) fetch(i + 1, &nd, &ne);  // in flight during this block
+            if (!mbar_wait(&empty[s], ((uint32_t)(i / kFStages) & 1u) ^ 1u)) *flag = 1;
+            unsigned char* base = tiles + (size_t)s * kFStage;
+            const double* srx = stage_rx(rbuf);
+            const double* srz = stage_rz(rbuf);
+            const float2* se = stage_e(rbuf);
+#pragma unroll 1
+            for (int cc = 0; cc < 4; ++cc) {
+                const int c = 4 * h + cc;
+                uint32_t ah[4], al[4], bh[4], bl[4];
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    const int j = 4 * c + jj;
+                    float ca = 0.f, sa = 0.f, wr = 0.f, wi = 0.f;
+                    if (va) phasor_t(zv, srz[j], g.a_turns, &ca, &sa);
+                    if (vb) {
+                        float cb, sb;
+                        phasor_t(xv, srx[j], g.a_turns, &cb, &sb);
+                        const float2 e = se[j];
+                        wr = e.x * cb - e.y * sb;
+                        wi = e.x * sb + e.y * cb;
+                    }
+                    split16x2(ca, sa, &ah[jj], &al[jj]);
+                    split16x2(wr, wi, &bh[jj], &bl[jj]);
+                }
+                // A row: (Re Z, Im Z); B rows 2r: (Re W, -Im W), 2r+1: (Im W, Re W).
+                *reinterpret_cast<uint4*>(base + sw128(r, c)) = make_uint4(ah[0], ah[1], ah[2], ah[3]);
+                *reinterpret_cast<uint4*>(base + kFA + sw128(r, c)) =
+                    make_uint4(al[0], al[1], al[2], al[3]);
+                unsigned char* bhi = base + 2 * kFA;
+                unsigned char* blo = bhi + kFB;
+                // Rows 2r and 2r+1, the first store to row 2r + sel: eight
+                // consecutive threads then hit eight distinct swizzle phases.
+                const int sel = (r >> 2) & 1;
+                const uint4 e0h = make_uint4(neg_hi(bh[0]), neg_hi(bh[1]), neg_hi(bh[2]), neg_hi(bh[3]));
+                const uint4 e1h = make_uint4(swap_halves(bh[0]), swap_halves(bh[1]),
+                                             swap_halves(bh[2]), swap_halves(bh[3]));
+                const uint4 e0l = make_uint4(neg_hi(bl[0]), neg_hi(bl[1]), neg_hi(bl[2]), neg_hi(bl[3]));
+                const uint4 e1l = make_uint4(swap_halves(bl[0]), swap_halves(bl[1]),
+                                             swap_halves(bl[2]), swap_halves(bl[3]));
+                *reinterpret_cast<uint4*>(bhi + sw128(2 * r + sel, c)) = sel ? e1h : e0h;
+                *reinterpret_cast<uint4*>(bhi + sw128(2 * r + 1 - sel, c)) = sel ? e0h : e1h;
+                *reinterpret_cast<uint4*>(blo + sw128(2 * r + sel, c)) = sel ? e1l : e0l;
+                *reinterpret_cast<uint4*>(blo + sw128(2 * r + 1 - sel, c)) = sel ? e0l : e1l;
+            }
+            // Make the generic-proxy stores visible to the tensor cores, then
+            // one arrival per warp.
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&full[s]);
+            if (i + 1 < nrb) put(rbuf ^ 1, nd, ne);
+            producer_sync();
+        }
     }
     __syncthreads();
-    if (*flag != 0 && threadIdx.x == 0) atomicExch(err, 1);
+    if (*flag != 0 && threadIdx.x == 0) atomicExch(g.err, 1);
     tc_fence_before();
     __syncthreads();
-    if (warp == 1) {
+    if (warp == 0) {
         tc_fence_after();
-        tmem_free(tmem, 2 * kBN);
+        tmem_free(tmem, 2 * kFN);
     }
 }
 
@@ -361,57 +417,19 @@ size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 unsigned grid_1d(size_t n, unsigned threads) { return (unsigned)((n + threads - 1) / threads); }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    });
-    return fn;
-}
-
-// Row-major [rows][k] f16 matrix, tiles of box_rows x 64 with the 128-byte swizzle.
-Status make_map(CUtensorMap* map, const void* base, size_t k, size_t rows, uint32_t box_rows) {
-    auto fn = encode_fn();
-    if (!fn) return Status::Err(XK_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(k * 2)};
-    cuuint32_t box[2] = {(cuuint32_t)kBK, box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides,
-                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return Status::Err(XK_ERR_CUDA, "tensor map encoding failed");
-    return Status::Ok();
-}
-
 }  // namespace
 
-FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms, size_t factor_budget,
-                           size_t max_chunk_rays) {
+FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms) {
     FresnelShape sh;
-    sh.m_pad = round_up(std::max<size_t>(nz, 1), kBM);
-    sh.n_pad = round_up(std::max<size_t>(2 * nx, 1), kBN);
-    // Rays per chunk: a multiple of 32 (K3 = 6 kc is then a multiple of the
-    // 64-wide K block) within the factor-memory budget.
-    const size_t per_ray = 12 * (sh.m_pad + sh.n_pad);  // bytes of A and B per ray
-    size_t kc = std::max<size_t>(32, factor_budget / per_ray / 32 * 32);
-    if (max_chunk_rays) kc = std::min(kc, std::max<size_t>(32, max_chunk_rays / 32 * 32));
-    kc = std::min(kc, round_up(std::max<size_t>(n, 1), 32));
-    sh.kc = kc;
-    sh.chunks = (n + kc - 1) / kc;
-    sh.k3 = 6 * kc;
-    sh.kb_total = (int)(sh.k3 / kBK);
-    const size_t tiles = (sh.m_pad / kBM) * (sh.n_pad / kBN);
-    size_t splits = tiles >= (size_t)num_sms ? 1 : (size_t)num_sms / tiles;
-    splits = std::max<size_t>(1, std::min(splits, (size_t)std::max(1, sh.kb_total / 4)));
-    sh.splits = (int)splits;
-    sh.tiles = tiles;
+    sh.m_pad = round_up(std::max<size_t>(nz, 1), 128);
+    sh.n_pad = round_up(std::max<size_t>(2 * nx, 1), kFN);
+    sh.ray_blocks = (int)((n + kFRays - 1) / kFRays);
+    sh.tiles = (sh.m_pad / 128) * (sh.n_pad / kFN);
+    // K splits: about one CTA per SM over the output tiles, each split at
+    // least a few accumulation segments long.
+    size_t splits = sh.tiles >= (size_t)num_sms ? 1 : (size_t)num_sms / sh.tiles;
+    splits = std::min(splits, std::max<size_t>(1, (size_t)sh.ray_blocks / (2 * kFSeg)));
+    sh.splits = (int)std::max<size_t>(1, splits);
     return sh;
 }
 
@@ -435,55 +453,52 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
         rep->kernels += 1;
         return Status::Ok();
     }
-    const FresnelShape sh = fresnel_shape(n, nx, nz, num_sms, ws.factor_budget, ws.max_chunk_rays);
-    XK_TRY(ws.factors.ensure((sh.m_pad + sh.n_pad) * sh.k3 * sizeof(__half)));
+    const FresnelShape sh = fresnel_shape(n, nx, nz, num_sms);
     XK_TRY(ws.partial.ensure((size_t)sh.splits * sh.m_pad * sh.n_pad * sizeof(double)));
     XK_TRY(ws.ctrl.ensure(256));
-    __half* A = ws.factors.as<__half>();
-    __half* B = A + sh.m_pad * sh.k3;
-    CUtensorMap mapA, mapB;
-    XK_TRY(make_map(&mapA, A, sh.k3, sh.m_pad, kBM));
-    XK_TRY(make_map(&mapB, B, sh.k3, sh.n_pad, kBN));
     static std::once_flag attr_once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(fresnel_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kGemmSmem);
+        attr_err = cudaFuncSetAttribute(fresnel_fused_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmem);
     });
     XK_CUDA_TRY(attr_err);
     int* d_err = ws.ctrl.as<int>();
     XK_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
-    // Padding rows of A and B stay zero for every chunk.
-    XK_CUDA_TRY(cudaMemsetAsync(ws.factors.ptr, 0, (sh.m_pad + sh.n_pad) * sh.k3 * sizeof(__half),
-                                stream));
-    const double inv_scale = 1.0 / in.max_amp;
-    const dim3 grid((unsigned)(sh.m_pad / kBM), (unsigned)(sh.n_pad / kBN), (unsigned)sh.splits);
-    for (size_t c = 0; c < sh.chunks; ++c) {
-        const size_t j0 = c * sh.kc;
-        factor_a_kernel<<<grid_1d(nz * sh.kc, 256), 256, 0, stream>>>(zp, nz, in.rz, n, j0, sh.kc,
-                                                                       pre, A, sh.k3);
-        factor_b_kernel<<<grid_1d(nx * sh.kc, 256), 256, 0, stream>>>(
-            xp, nx, in.rx, in.er, in.ei, n, j0, sh.kc, pre, inv_scale, B, sh.k3);
-        XK_CUDA_TRY(cudaGetLastError());
-        const bool timed = rep->ev_gemm[0] && rep->ev_gemm[1];
-        if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[0], stream));
-        fresnel_gemm_kernel<<<grid, kGemmThreads, kGemmSmem, stream>>>(
-            mapA, mapB, sh.kb_total, sh.splits, ws.partial.as<double>(), (int)sh.m_pad,
-            (int)sh.n_pad, d_err);
-        XK_CUDA_TRY(cudaGetLastError());
-        if (timed) {
-            XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[1], stream));
-            XK_CUDA_TRY(cudaEventSynchronize(rep->ev_gemm[1]));
-            float ms = 0.f;
-            XK_CUDA_TRY(cudaEventElapsedTime(&ms, rep->ev_gemm[0], rep->ev_gemm[1]));
-            rep->gemm_ms += ms;
-        }
-        reduce_kernel<<<grid_1d(m, 256), 256, 0, stream>>>(ws.partial.as<double>(), sh.splits,
-                                                            (int)sh.m_pad, (int)sh.n_pad, nz, nx,
-                                                            in.max_amp, in.out_re, in.out_im,
-                                                            c == 0);
-        XK_CUDA_TRY(cudaGetLastError());
-        rep->kernels += 4;
+    FusedArgs fa;
+    fa.rx = in.rx;
+    fa.rz = in.rz;
+    fa.er = in.er;
+    fa.ei = in.ei;
+    fa.n = n;
+    fa.ray_blocks = sh.ray_blocks;
+    fa.splits = sh.splits;
+    fa.xp = xp;
+    fa.zp = zp;
+    fa.nx = nx;
+    fa.nz = nz;
+    fa.a_turns = pre * kInv2Pi;
+    fa.inv_scale = 1.0 / in.max_amp;
+    fa.partial = ws.partial.as<double>();
+    fa.m_pad = (int)sh.m_pad;
+    fa.n_pad = (int)sh.n_pad;
+    fa.err = d_err;
+    const dim3 grid((unsigned)(sh.m_pad / 128), (unsigned)(sh.n_pad / kFN), (unsigned)sh.splits);
+    const bool timed = rep->ev_gemm[0] && rep->ev_gemm[1];
+    if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[0], stream));
+    fresnel_fused_kernel<<<grid, kFThreads, kFSmem, stream>>>(fa);
+    XK_CUDA_TRY(cudaGetLastError());
+    if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[1], stream));
+    reduce_kernel<<<grid_1d(m, 256), 256, 0, stream>>>(ws.partial.as<double>(), sh.splits,
+                                                        (int)sh.m_pad, (int)sh.n_pad, nz, nx,
+                                                        in.max_amp, in.out_re, in.out_im, 1);
+    XK_CUDA_TRY(cudaGetLastError());
+    rep->kernels += 2;
+    if (timed) {
+        XK_CUDA_TRY(cudaEventSynchronize(rep->ev_gemm[1]));
+        float ms = 0.f;
+        XK_CUDA_TRY(cudaEventElapsedTime(&ms, rep->ev_gemm[0], rep->ev_gemm[1]));
+        rep->gemm_ms += ms;
     }
     rep->shape = sh;
     rep->d_err = d_err;
@@ -566,10 +581,10 @@ xk::Status fresnel_host(xk_ctx* ctx, const double* rx, const double* rz, const d
         stats->pairs = (double)n * (double)m;
         stats->h2d_bytes = 4.0 * nb;
         stats->d2h_bytes = 2.0 * m * sizeof(double) + (double)(nx + nz) * sizeof(double);
-        stats->n_chunks = (int)rep.shape.chunks;
+        stats->n_chunks = rep.shape.ray_blocks;
         stats->n_tiles = (int)rep.shape.tiles;
         stats->groups = rep.shape.splits;
-        stats->n_items = (long long)rep.shape.tiles * rep.shape.splits * (long long)rep.shape.chunks;
+        stats->n_items = (long long)rep.shape.tiles * rep.shape.splits;
         stats->sweep = -1;
     }
     return xk::Status::Ok();

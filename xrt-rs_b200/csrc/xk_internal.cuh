@@ -140,16 +140,14 @@ struct FresnelIn {
 };
 
 struct FresnelShape {
-    size_t m_pad = 0, n_pad = 0;  // padded rows of the A (screen z) and B (2 x screen x) factors
-    size_t kc = 0, k3 = 0;        // rays per chunk, f16 columns per factor row (6 kc)
-    size_t chunks = 0, tiles = 0;
-    int kb_total = 0, splits = 1; // 64-wide K blocks per chunk, K splits per output tile
+    size_t m_pad = 0, n_pad = 0;  // padded rows of A (screen z) and B (2 x screen x)
+    size_t tiles = 0;             // 128 x 256 output tiles
+    int ray_blocks = 0;           // blocks of 32 rays (the contraction)
+    int splits = 1;               // K splits per output tile
 };
 
 struct FresnelWorkspace {
-    DevBuf coords, factors, partial, ctrl;
-    size_t factor_budget = size_t(2) << 30;  // bytes of f16 factors per ray chunk
-    size_t max_chunk_rays = 0;               // cap on rays per chunk (0 = budget only)
+    DevBuf coords, partial, ctrl;
 };
 
 struct FresnelReport {
@@ -160,8 +158,7 @@ struct FresnelReport {
     int* d_err = nullptr;                       // device error word of the products
 };
 
-FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms, size_t factor_budget,
-                           size_t max_chunk_rays);
+FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms);
 
 // Enqueues screen coordinates into ws.coords (nx then nz doubles; the caller
 // sizes it) and the sum for `path` (XK_PATH_F64 or XK_PATH_SEPARABLE).
