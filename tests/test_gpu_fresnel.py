@@ -139,3 +139,16 @@ def test_separable_long_accumulation_against_f64(ctx):
     print(f"long K: rel L2 {err:.2e}, tiles {st['n_tiles']} x splits {st['groups']}")
     assert st["groups"] <= 4
     assert err < 1e-5
+
+
+def test_separable_routes_to_f64_beyond_the_cross_term_bound(ctx, oracle):
+    """A screen of +-50 mm at 30 keV and 100 mm puts the FP32 cross term of the
+    phase split beyond 2^21 turns: the call runs the FP64 sum instead and
+    reports it."""
+    rng = np.random.default_rng(21)
+    x, z = rng.uniform(-1, 1, 300), rng.uniform(-1, 1, 300)
+    es = np.exp(1j * rng.uniform(-np.pi, np.pi, 300))
+    sc = FresnelScreen(-50.0, 50.0, 9, -50.0, 50.0, 7)
+    res, st = xrt_rs.fresnel_propagate(x, z, es, 30000.0, 100.0, sc, ctx=ctx, return_stats=True)
+    assert st["path"] == xrt_rs._lib.XK_PATH_F64
+    assert rel(res.amplitude, oracle_field(oracle, x, z, es, 30000.0, 100.0, sc)) < F64_TOL

@@ -118,9 +118,13 @@ constexpr int kFProdThreads = 256;               // warps 5..12
 constexpr int kFThreads = 32 + kFEpiThreads + kFProdThreads;
 constexpr int kFSeg = 20;                        // ray blocks (60 K blocks) per f32 segment
 constexpr int kFN = 256;                         // accumulator columns (N of the UMMA)
-// Ray staging (two blocks): rx, rz (f64) and the scaled amplitude (f32 x 2).
-constexpr uint32_t kFRayBytes = kFRays * (8 + 8 + 8);
-constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + 2 * kFRayBytes + 256;
+// Ray staging (two blocks), per ray 8 floats: x hi, x lo, frac(a x^2), z hi,
+// z lo, frac(a z^2) (coordinates relative to the screen centre) and the
+// scaled amplitude.
+constexpr uint32_t kFRayBytes = kFRays * 32;
+// Epilogue transpose buffers: per epilogue warp 32 x 33 floats.
+constexpr uint32_t kFEpiBytes = 4 * 32 * 33 * 4;
+constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + 2 * kFRayBytes + kFEpiBytes + 256;
 
 struct FusedArgs {
     const double *rx, *rz, *er, *ei;
@@ -130,6 +134,7 @@ struct FusedArgs {
     size_t nx, nz;
     double a_turns;    // k / (2 d) / (2 pi)
     double inv_scale;  // 1 / max|es|
+    double ox, oz;     // origin of the phase split (screen centre)
     double* partial;   // [splits][m_pad][n_pad]
     int m_pad, n_pad;
     int* err;
@@ -140,12 +145,36 @@ __device__ __forceinline__ uint32_t sw128(uint32_t r, uint32_t c) {
     return r * 128u + ((c ^ (r & 7u)) << 4);
 }
 
-// exp(2 pi i t), t = a_turns (p - r)^2 in turns, reduced in FP64.
-__device__ __forceinline__ void phasor_t(double p, double r, double a_turns, float* c, float* s) {
-    const double d = p - r;
-    const double t = (a_turns * d) * d;
-    const float f = (float)(t - rint(t));
-    __sincosf(6.28318530717958647692f * f, s, c);
+// Phase split. With p, r relative to the screen centre the phase in turns is
+//     t = a (p - r)^2 = P(p) + kappa(p) r + R(r),
+//     P = frac(a p^2), R = frac(a r^2), kappa = -2 a p,
+// where P and R are reduced in FP64 once per screen row and per ray. The
+// cross term kappa r (up to 2^21 turns, checked on the host) is formed
+// exactly in FP32 from hi/lo splits of kappa and r: the rounded product
+// kh*rh, its FMA error term, and the two small cross products; its integer
+// part drops out and the fractional remainder keeps ~1e-7 turn.
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: (x + kMagic) - kMagic = rint(x), |x| < 2^22
+
+__device__ __forceinline__ float round_nearest(float x) {
+    return __fsub_rn(__fadd_rn(x, kMagic), kMagic);
+}
+
+__device__ __forceinline__ float pair_turns(float kh, float kl, float pr, float rh, float rl) {
+    const float p1 = __fmul_rn(kh, rh);
+    const float e1 = __fmaf_rn(kh, rh, -p1);
+    const float f1 = __fsub_rn(p1, round_nearest(p1));
+    float sm = __fmaf_rn(kh, rl, e1);
+    sm = __fmaf_rn(kl, rh, sm);
+    const float t = __fadd_rn(__fadd_rn(pr, f1), sm);
+    return __fsub_rn(t, round_nearest(t));
+}
+
+// hi/lo float split of a double and frac(a v^2) as a float.
+__device__ __forceinline__ void split_coord(double v, double a, float* hi, float* lo, float* fr) {
+    *hi = (float)v;
+    *lo = (float)(v - (double)*hi);
+    const double t = (a * v) * v;
+    *fr = (float)(t - rint(t));
 }
 
 // (a, b) -> f16x2 hi (round to nearest) and f16x2 lo = (a, b) - hi.
@@ -243,13 +272,17 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
         }
         __syncwarp();
     } else if (warp <= 4) {
-        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31.
+        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, i.e. rows
+        // qd*32 .. +31 of the tile. Each 32 x 32 block of the accumulator is
+        // transposed through shared memory so that the FP64 partial is
+        // updated one row at a time, 32 consecutive columns per access.
         const int qd = warp & 3;
-        const int row = mt * 128 + qd * 32 + lane;
-        double* dst = g.partial + ((size_t)sp * g.m_pad + row) * g.n_pad + (size_t)nt * kFN;
+        float* tb = reinterpret_cast<float*>(rays_smem + 2 * kFRayBytes) + (warp - 1) * 32 * 33;
+        double* rows0 = g.partial + ((size_t)sp * g.m_pad + (size_t)mt * 128 + qd * 32) * g.n_pad +
+                        (size_t)nt * kFN + lane;
         if (nseg == 0)
-            for (int c = 0; c < kFN; c += 2)
-                *reinterpret_cast<double2*>(dst + c) = make_double2(0.0, 0.0);
+            for (int rr = 0; rr < 32; ++rr)
+                for (int c = 0; c < kFN; c += 32) rows0[(size_t)rr * g.n_pad + c] = 0.0;
         for (int q = 0; q < nseg; ++q) {
             const int b = q & 1;
             const bool ok = mbar_wait(&acc_full[b], (uint32_t)(q >> 1) & 1u);
@@ -262,20 +295,18 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             for (int c = 0; c < kFN / 32; ++c) {
                 float v[32];
                 tmem_ld_32cols(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * kFN + c * 32), v);
-                double2* d2 = reinterpret_cast<double2*>(dst + c * 32);
+#pragma unroll
+                for (int k = 0; k < 32; ++k) tb[lane * 33 + k] = v[k];
+                __syncwarp();
+                double* d = rows0 + c * 32;
                 if (q == 0) {
-#pragma unroll
-                    for (int t = 0; t < 16; ++t)
-                        d2[t] = make_double2((double)v[2 * t], (double)v[2 * t + 1]);
+#pragma unroll 8
+                    for (int rr = 0; rr < 32; ++rr) d[(size_t)rr * g.n_pad] = (double)tb[rr * 33 + lane];
                 } else {
-#pragma unroll
-                    for (int t = 0; t < 16; ++t) {
-                        double2 o = d2[t];
-                        o.x += (double)v[2 * t];
-                        o.y += (double)v[2 * t + 1];
-                        d2[t] = o;
-                    }
+#pragma unroll 8
+                    for (int rr = 0; rr < 32; ++rr) d[(size_t)rr * g.n_pad] += (double)tb[rr * 33 + lane];
                 }
+                __syncwarp();
             }
             tc_fence_before();
             mbar_arrive(&acc_empty[b]);
@@ -290,43 +321,53 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
         const int h = p >> 7, r = p & 127;
         const size_t iz = (size_t)mt * 128 + r, ix = (size_t)nt * 128 + r;
         const bool va = iz < g.nz, vb = ix < g.nx;
-        const double zv = va ? g.zp[iz] : 0.0, xv = vb ? g.xp[ix] : 0.0;
-        auto stage_rx = [&](int buf) { return reinterpret_cast<double*>(rays_smem + buf * kFRayBytes); };
-        auto stage_rz = [&](int buf) { return stage_rx(buf) + kFRays; };
-        auto stage_e = [&](int buf) { return reinterpret_cast<float2*>(stage_rx(buf) + 2 * kFRays); };
-        // Value this thread stages for block `blk` (threads 0..95 only).
-        auto fetch = [&](int blk, double* dv, float2* ev) {
-            const size_t j = (size_t)(rb0 + blk) * kFRays + (p & 31);
-            const bool in = j < g.n;
-            if (p < 32) *dv = in ? __ldg(g.rx + j) : 0.0;
-            else if (p < 64) *dv = in ? __ldg(g.rz + j) : 0.0;
-            else if (p < 96)
-                *ev = in ? make_float2((float)(__ldg(g.er + j) * g.inv_scale),
-                                       (float)(__ldg(g.ei + j) * g.inv_scale))
-                         : make_float2(0.f, 0.f);
+        // Per-row terms: kappa = -2 a p (hi, lo) and P = frac(a p^2).
+        float kzh = 0.f, kzl = 0.f, pz = 0.f, kxh = 0.f, kxl = 0.f, px = 0.f;
+        {
+            const double zr = va ? g.zp[iz] - g.oz : 0.0, xr = vb ? g.xp[ix] - g.ox : 0.0;
+            float unused;
+            split_coord(-2.0 * g.a_turns * zr, 0.0, &kzh, &kzl, &unused);
+            split_coord(-2.0 * g.a_turns * xr, 0.0, &kxh, &kxl, &unused);
+            float h0, l0;
+            split_coord(zr, g.a_turns, &h0, &l0, &pz);
+            split_coord(xr, g.a_turns, &h0, &l0, &px);
+        }
+        auto stage = [&](int buf) { return reinterpret_cast<float4*>(rays_smem + buf * kFRayBytes); };
+        // Ray values of block `blk` (threads 0..31, one ray each).
+        auto fetch = [&](int blk, float4* v0, float4* v1) {
+            const size_t j = (size_t)(rb0 + blk) * kFRays + p;
+            if (p >= 32) return;
+            if (j >= g.n) {
+                *v0 = make_float4(0.f, 0.f, 0.f, 0.f);
+                *v1 = make_float4(0.f, 0.f, 0.f, 0.f);
+                return;
+            }
+            float xh, xl, xf, zh, zl, zf;
+            split_coord(__ldg(g.rx + j) - g.ox, g.a_turns, &xh, &xl, &xf);
+            split_coord(__ldg(g.rz + j) - g.oz, g.a_turns, &zh, &zl, &zf);
+            *v0 = make_float4(xh, xl, xf, zh);
+            *v1 = make_float4(zl, zf, (float)(__ldg(g.er + j) * g.inv_scale),
+                              (float)(__ldg(g.ei + j) * g.inv_scale));
         };
-        auto put = [&](int buf, double dv, float2 ev) {
-            if (p < 32) stage_rx(buf)[p] = dv;
-            else if (p < 64) stage_rz(buf)[p - 32] = dv;
-            else if (p < 96) stage_e(buf)[p - 64] = ev;
+        auto put = [&](int buf, float4 v0, float4 v1) {
+            if (p < 32) {
+                stage(buf)[2 * p] = v0;
+                stage(buf)[2 * p + 1] = v1;
+            }
         };
         if (nrb > 0) {
-            double dv = 0.0;
-            float2 ev = make_float2(0.f, 0.f);
-            fetch(0, &dv, &ev);
-            put(0, dv, ev);
+            float4 v0, v1;
+            fetch(0, &v0, &v1);
+            put(0, v0, v1);
         }
         producer_sync();
         for (int i = 0; i < nrb; ++i) {
             const int s = i % kFStages, rbuf = i & 1;
-            double nd = 0.0;
-            float2 ne = make_float2(0.f, 0.f);
-            if (i + 1 < nrb) fetch(i + 1, &nd, &ne);  // in flight during this block
+            float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0;
+            if (i + 1 < nrb) fetch(i + 1, &n0, &n1);  // in flight during this block
             if (!mbar_wait(&empty[s], ((uint32_t)(i / kFStages) & 1u) ^ 1u)) *flag = 1;
             unsigned char* base = tiles + (size_t)s * kFStage;
-            const double* srx = stage_rx(rbuf);
-            const double* srz = stage_rz(rbuf);
-            const float2* se = stage_e(rbuf);
+            const float4* sr = stage(rbuf);
 #pragma unroll 1
             for (int cc = 0; cc < 4; ++cc) {
                 const int c = 4 * h + cc;
@@ -334,14 +375,18 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
 #pragma unroll
                 for (int jj = 0; jj < 4; ++jj) {
                     const int j = 4 * c + jj;
+                    const float4 v0 = sr[2 * j], v1 = sr[2 * j + 1];
                     float ca = 0.f, sa = 0.f, wr = 0.f, wi = 0.f;
-                    if (va) phasor_t(zv, srz[j], g.a_turns, &ca, &sa);
+                    if (va) {
+                        const float t = pair_turns(kzh, kzl, __fadd_rn(pz, v1.y), v0.w, v1.x);
+                        __sincosf(6.28318530717958647692f * t, &sa, &ca);
+                    }
                     if (vb) {
                         float cb, sb;
-                        phasor_t(xv, srx[j], g.a_turns, &cb, &sb);
-                        const float2 e = se[j];
-                        wr = e.x * cb - e.y * sb;
-                        wi = e.x * sb + e.y * cb;
+                        const float t = pair_turns(kxh, kxl, __fadd_rn(px, v0.z), v0.x, v0.y);
+                        __sincosf(6.28318530717958647692f * t, &sb, &cb);
+                        wr = v1.z * cb - v1.w * sb;
+                        wi = v1.z * sb + v1.w * cb;
                     }
                     split16x2(ca, sa, &ah[jj], &al[jj]);
                     split16x2(wr, wi, &bh[jj], &bl[jj]);
@@ -371,7 +416,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&full[s]);
-            if (i + 1 < nrb) put(rbuf ^ 1, nd, ne);
+            if (i + 1 < nrb) put(rbuf ^ 1, n0, n1);
             producer_sync();
         }
     }
@@ -444,6 +489,14 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     rep->kernels += 2;
     const double k = in.energy / kChbar * 1e7;
     const double pre = k / (2.0 * in.dist);
+    // Origin of the phase split and the bound on its FP32 cross term.
+    const double ox = 0.5 * (in.x_min + in.x_max), oz = 0.5 * (in.z_min + in.z_max);
+    const double cross = 2.0 * pre * kInv2Pi *
+                         std::max(0.5 * std::fabs(in.x_max - in.x_min) * in.max_rx_off,
+                                  0.5 * std::fabs(in.z_max - in.z_min) * in.max_rz_off);
+    rep->used_path = path;
+    if (path == XK_PATH_SEPARABLE && n && in.max_amp != 0.0 && !(cross < 2097152.0))
+        rep->used_path = path = XK_PATH_F64;
     if (path == XK_PATH_F64 || n == 0 || in.max_amp == 0.0) {
         // FP64 direct sum (with no rays or zero amplitudes it writes zeros).
         const size_t nn = (path == XK_PATH_F64) ? n : 0;
@@ -479,6 +532,8 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     fa.nz = nz;
     fa.a_turns = pre * kInv2Pi;
     fa.inv_scale = 1.0 / in.max_amp;
+    fa.ox = ox;
+    fa.oz = oz;
     fa.partial = ws.partial.as<double>();
     fa.m_pad = (int)sh.m_pad;
     fa.n_pad = (int)sh.n_pad;
@@ -531,11 +586,17 @@ xk::Status fresnel_host(xk_ctx* ctx, const double* rx, const double* rz, const d
     const double* src[4] = {rx, rz, er, ei};
     for (int f = 0; f < 4 && n; ++f)
         XK_CUDA_TRY(cudaMemcpyAsync(d + f * n, src[f], nb, cudaMemcpyHostToDevice, s));
-    double max_amp = 0.0;
-    for (size_t j = 0; j < n; ++j) max_amp = std::max(max_amp, std::hypot(er[j], ei[j]));
+    double max_amp = 0.0, max_rx = 0.0, max_rz = 0.0;
+    const double ox = 0.5 * (sc->x_min + sc->x_max), oz = 0.5 * (sc->z_min + sc->z_max);
+    for (size_t j = 0; j < n; ++j) {
+        max_amp = std::max(max_amp, std::hypot(er[j], ei[j]));
+        max_rx = std::max(max_rx, std::fabs(rx[j] - ox));
+        max_rz = std::max(max_rz, std::fabs(rz[j] - oz));
+    }
     double* out = ctx->out_field.as<double>();
     xk::FresnelIn in{d, d + n, d + 2 * n, d + 3 * n, n, energy, dist,
-                     sc->x_min, sc->x_max, sc->z_min, sc->z_max, nx, nz, max_amp, out, out + m};
+                     sc->x_min, sc->x_max, sc->z_min, sc->z_max, nx, nz, max_amp, max_rx, max_rz,
+                     out, out + m};
     xk::FresnelReport rep;
     cudaEvent_t g0 = nullptr, g1 = nullptr;
     if (stats && path == XK_PATH_SEPARABLE) {
@@ -577,7 +638,7 @@ xk::Status fresnel_host(xk_ctx* ctx, const double* rx, const double* rz, const d
         stats->gpu_ms = ms;
         stats->main_kernel_ms = rep.gemm_ms;
         stats->kernels = rep.kernels;
-        stats->path = path;
+        stats->path = rep.used_path;
         stats->pairs = (double)n * (double)m;
         stats->h2d_bytes = 4.0 * nb;
         stats->d2h_bytes = 2.0 * m * sizeof(double) + (double)(nx + nz) * sizeof(double);

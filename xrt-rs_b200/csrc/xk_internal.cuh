@@ -136,6 +136,7 @@ struct FresnelIn {
     double x_min, x_max, z_min, z_max;
     size_t nx, nz;
     double max_amp;                   // max_j |es_j| (scales the f16 factors)
+    double max_rx_off, max_rz_off;    // max_j |x_j - screen centre x|, same for z
     double *out_re, *out_im;          // device, nx * nz each
 };
 
@@ -156,6 +157,7 @@ struct FresnelReport {
     cudaEvent_t ev_gemm[2] = {nullptr, nullptr};  // set to time the products (synchronises per chunk)
     FresnelShape shape;
     int* d_err = nullptr;                       // device error word of the products
+    int used_path = 0;                          // XK_PATH_* that ran
 };
 
 FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms);
