@@ -300,11 +300,16 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
                 __syncwarp();
                 double* d = rows0 + c * 32;
                 if (q == 0) {
-#pragma unroll 8
+#pragma unroll
                     for (int rr = 0; rr < 32; ++rr) d[(size_t)rr * g.n_pad] = (double)tb[rr * 33 + lane];
                 } else {
-#pragma unroll 8
-                    for (int rr = 0; rr < 32; ++rr) d[(size_t)rr * g.n_pad] += (double)tb[rr * 33 + lane];
+                    // All 32 loads in flight before the adds.
+                    double old[32];
+#pragma unroll
+                    for (int rr = 0; rr < 32; ++rr) old[rr] = d[(size_t)rr * g.n_pad];
+#pragma unroll
+                    for (int rr = 0; rr < 32; ++rr)
+                        d[(size_t)rr * g.n_pad] = old[rr] + (double)tb[rr * 33 + lane];
                 }
                 __syncwarp();
             }
