@@ -7,7 +7,7 @@ output order (index iz * nx + ix). The sum runs in libxk.so:
 * ``path="separable"`` (default): the Fresnel kernel factorises over the
   regular screen, so the whole screen is one complex matrix product over the
   rays, computed on the tensor cores from FP64 phasors split into f16
-  hi + lo parts (relative L2 error ~1e-6 against the FP64 sum);
+  hi + lo parts (relative L2 error ~5e-6 against the FP64 sum);
 * ``path="f64"``: the reference's FP64 sum, term for term.
 """
 from __future__ import annotations
