@@ -102,6 +102,13 @@ xk::Status create_batch(xk_ctx* ctx, const xk_solve* solves, size_t n, int path,
     XK_CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     XK_CUDA_TRY(cudaEventCreate(&b->ev0));
     XK_CUDA_TRY(cudaEventCreate(&b->ev1));
+    // Stream-ordered allocations from the device pool: a batch created after
+    // another one reuses its memory instead of mapping new memory.
+    XK_TRY(xk::keep_pool_memory(ctx->device));
+    b->ws.set_async(b->stream);
+    b->inputs.async_stream = b->stream;
+    b->f64ws.rays.async_stream = b->stream;
+    b->f64ws.partials.async_stream = b->stream;
     const bool device = (flags & XK_BATCH_DEVICE) != 0;
 
     // Device views of every solve; host inputs are copied once into one buffer.

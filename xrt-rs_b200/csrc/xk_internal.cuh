@@ -44,6 +44,17 @@ struct Status {
         if (!st__.ok()) return st__;      \
     } while (0)
 
+// Keeps memory freed to the device's default stream-ordered pool in the pool
+// (instead of returning it to the driver at every synchronisation), so that
+// repeated batch and server allocations of similar sizes are reused.
+inline Status keep_pool_memory(int device) {
+    cudaMemPool_t pool;
+    XK_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t threshold = UINT64_MAX;
+    XK_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    return Status::Ok();
+}
+
 // A growable device buffer (never shrinks until freed). With `async_stream`
 // set it allocates and frees stream-ordered (cudaMallocAsync/cudaFreeAsync on
 // that stream), which never waits for other streams' work.

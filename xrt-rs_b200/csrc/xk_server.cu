@@ -614,10 +614,7 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
     s->pr_opts = ctx->pr_opts;
     // Keep freed stream-ordered memory in the pool instead of returning it to
     // the driver at every synchronisation.
-    cudaMemPool_t pool;
-    XK_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
-    uint64_t threshold = UINT64_MAX;
-    XK_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    XK_TRY(xk::keep_pool_memory(ctx->device));
     int lo = 0, hi = 0;
     XK_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->plan_stream, cudaStreamNonBlocking, hi));
