@@ -105,6 +105,19 @@ def test_odd_sizes(ctx, oracle, n_rays, n_pix):
     assert cases.rel_l2(out32, ref) < PR_TOL
 
 
+def test_exhaustive_tiny_sizes(ctx, oracle):
+    """Every size of 1-7 rays x 1-9 screen points on both paths: the smallest
+    cases hit every partial warp, stage and tile edge."""
+    for n_rays in range(1, 8):
+        for n_pix in range(1, 10):
+            rays, pix = cases.random_case(n_rays, n_pix, seed=100 * n_rays + n_pix)
+            ref = oracle_run(oracle, rays, pix)
+            out64, _ = run(ctx, rays, pix, "f64")
+            assert cases.rel_l2(out64, ref) < F64_TOL, (n_rays, n_pix)
+            out32, _ = run(ctx, rays, pix, "f32pr")
+            assert cases.rel_l2(out32, ref) < PR_TOL, (n_rays, n_pix)
+
+
 def test_general_normals(ctx, oracle):
     rays, pix = cases.random_case(3000, 700, seed=11, general_normals=True)
     ref = oracle_run(oracle, rays, pix)

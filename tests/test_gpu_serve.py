@@ -124,13 +124,18 @@ def test_injected_allocation_failures_fail_only_their_request(ctx, oracle):
     srv.close()
 
 
-def test_f64_requests_through_the_server(ctx, oracle):
+def test_f64_requests_through_the_server(ctx, oracle, tmp_path):
     rays, pix = cases.random_case(1500, 200, seed=8)
-    srv = Server(ctx)
+    log = tmp_path / "requests.jsonl"
+    srv = Server(ctx, log=str(log))
     out = srv.wait(srv.submit(pix, rays=rays, path="f64"))
     assert srv.last_stats["path"] == xrt_rs.XK_PATH_F64
     assert cases.rel_l2(out, oracle.kahan_f64(*cases.as_lists(rays, pix))) < F64_TOL
     srv.close()
+    import json
+    rec = [json.loads(line) for line in log.read_text().splitlines()]
+    assert len(rec) == 1 and rec[0]["pairs"] == 1500 * 200 and rec[0]["rc"] == 0
+    assert {"queue_ms", "total_ms", "queue_depth", "admitted_bytes"} <= set(rec[0])
 
 
 def test_wait_timeout_and_shutdown_with_queued_requests(ctx):

@@ -91,6 +91,7 @@ xk::RaysDev to_dev(const xk_rays* r) {
 xk::Status run_solve(xk_ctx* ctx, const xk::RaysDev& rays, size_t n_rays, const xk::PixDev& pix,
                      size_t n_pix, const xk::FieldDev& out, int path, cudaStream_t stream,
                      xk_stats* stats, int* used_path) {
+    xk::NvtxRange nvtx_range("xk solve");
     xk::LaunchReport rep;
     XK_CUDA_TRY(cudaEventRecord(ctx->ev0, stream));
     int used = path;

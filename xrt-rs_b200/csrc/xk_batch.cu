@@ -93,6 +93,7 @@ xk::Status enqueue_batch(xk_batch* b) {
 
 xk::Status create_batch(xk_ctx* ctx, const xk_solve* solves, size_t n, int path, int flags,
                         xk_batch** out) {
+    xk::NvtxRange nvtx_range("xk batch plan");
     auto t0 = std::chrono::steady_clock::now();
     xk_batch* b = new xk_batch();
     b->ctx = ctx;
@@ -197,6 +198,7 @@ xk::Status create_batch(xk_ctx* ctx, const xk_solve* solves, size_t n, int path,
 }
 
 xk::Status run_batch(xk_batch* b, xk_batch_stats* stats) {
+    xk::NvtxRange nvtx_range("xk batch run");
     auto t0 = std::chrono::steady_clock::now();
     XK_CUDA_TRY(cudaEventRecord(b->ev0, b->stream));
     if (b->exec) {

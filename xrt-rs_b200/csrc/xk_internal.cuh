@@ -8,6 +8,8 @@
 #include <mutex>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/xk.h"
 
 namespace xk {
@@ -43,6 +45,16 @@ struct Status {
         ::xk::Status st__ = (expr);       \
         if (!st__.ok()) return st__;      \
     } while (0)
+
+// NVTX range for the enclosing scope (header-only NVTX v3: a no-op unless a
+// profiler is attached), so that planning, epochs and copies show up as
+// named ranges on a timeline.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Keeps memory freed to the device's default stream-ordered pool in the pool
 // (instead of returning it to the driver at every synchronisation), so that

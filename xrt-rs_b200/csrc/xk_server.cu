@@ -241,6 +241,7 @@ xk::Status launch_f64(xk_server* s, Req* q) {
 
 // Copies and plans a batch of admitted requests; runs on the planner thread.
 void plan_batch(xk_server* s, std::vector<Req*>& batch) {
+    xk::NvtxRange nvtx_range("xk server plan batch");
     std::vector<Req*> ok, pr;
     for (Req* q : batch) {
         xk::Status st = copy_inputs(s, q);
@@ -329,6 +330,7 @@ void retire_slot(xk_server* s, EpochSlot& e) {
 
 // Builds and launches one epoch over the planned FP32-PR requests.
 xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
+    xk::NvtxRange nvtx_range("xk server epoch");
     EpochSlot& e = s->slots[s->next_slot];
     s->next_slot = (s->next_slot + 1) % kEpochRing;
     retire_slot(s, e);
@@ -529,6 +531,7 @@ void finisher_loop(xk_server* s) {
             q = s->computed.front();
             s->computed.pop_front();
         }
+        xk::NvtxRange nvtx_range("xk server finish request");
         int status = q->status;
         if (q->done_ev) {
             cudaError_t e = cudaEventSynchronize(q->done_ev);

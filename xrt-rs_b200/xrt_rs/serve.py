@@ -6,10 +6,15 @@
     es_re, es_im, ep_re, ep_im = srv.wait(t)   # blocks; srv.last_stats has latencies
 
 Every request keeps its numpy buffers alive until it has been waited for.
+With ``log=path`` every waited-for request appends one JSON line (ticket,
+status, pairs, queue/plan/run/total ms, epochs, path) followed by the
+server's counters (queue depth, active requests, bytes admitted).
 """
 from __future__ import annotations
 
 import ctypes
+import json
+import time
 
 import numpy as np
 
@@ -20,8 +25,9 @@ from . import (PIXEL_FIELDS, RAY_FIELDS, XkError, _check_lengths, _f64, _path, _
 
 class Server:
     def __init__(self, ctx=None, hbm_budget_bytes=0.0, epoch_pairs=0.0, max_active=0,
-                 item_pairs=0.0, inject_alloc_failure_every=0, reserve_sms=0):
+                 item_pairs=0.0, inject_alloc_failure_every=0, reserve_sms=0, log=None):
         self._ctx = _require_ctx(ctx)
+        self._log = open(log, "a") if log else None
         opts = _lib.XkServerOpts(float(hbm_budget_bytes), float(epoch_pairs), int(max_active),
                                  float(item_pairs), int(inject_alloc_failure_every),
                                  int(reserve_sms))
@@ -85,6 +91,13 @@ class Server:
             raise XkError(rc, "wait timed out; the request is still running")
         keep, out = self._live.pop(ticket)
         self.last_stats = st.to_dict()
+        if self._log is not None:
+            rec = {"t": time.time(), "ticket": ticket, "rc": rc, **self.last_stats}
+            srv = self.stats()
+            rec.update({"queue_depth": srv["pending"], "active": srv["active"],
+                        "admitted_bytes": srv["used_bytes"]})
+            self._log.write(json.dumps(rec) + "\n")
+            self._log.flush()
         _lib.check(rc)
         return out
 
@@ -99,6 +112,9 @@ class Server:
             self._h = None
         self._live.clear()
         self._sets.clear()
+        if getattr(self, "_log", None) is not None:
+            self._log.close()
+            self._log = None
 
     def __del__(self):
         try:
