@@ -447,7 +447,7 @@ struct PackedState {
 // evaluated in double-double arithmetic (error-free products by FMA, TwoSum,
 // one Newton correction of the square root).
 __device__ __forceinline__ double dd_turns(double kt_hi, double kt_lo, double qx, double qy,
-                                           double qz) {
+                                           double qz, double* qn) {
     const double p0 = qx * qx, p1 = qy * qy, p2 = qz * qz;
     const double e0 = fma(qx, qx, -p0), e1 = fma(qy, qy, -p1), e2 = fma(qz, qz, -p2);
     double s1 = p0 + p1;
@@ -460,6 +460,7 @@ __device__ __forceinline__ double dd_turns(double kt_hi, double kt_lo, double qx
     double hi = s2 + lo;
     lo -= hi - s2;
     const double r = sqrt(hi);
+    *qn = r;
     const double rl = (fma(-r, r, hi) + lo) / (2.0 * r);
     const double ph = kt_hi * r;
     const double pe = fma(kt_hi, r, -ph) + (kt_hi * rl + kt_lo * r);
@@ -487,12 +488,24 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
     for (int i = 0; i < kPrPpl; ++i) {
         const long long s = (long long)t * kPrTile + lane + 32 * i;
         double qx = sv.tpx[s] - r0x, qy = sv.tpy[s] - r0y, qz = sv.tpz[s] - r0z;
-        double qn = sqrt(qx * qx + qy * qy + qz * qz);
+        // Base phase k|q| in turns, carried in double-double (k|q| reaches
+        // 1e12 rad at 30 keV and 20 m, where one FP64 rounding is 1e-4 rad);
+        // the same square root gives |q|.
+        double qn;
+        const float fr = (float)dd_turns(sv.kt, sv.kt_lo, qx, qy, qz, &qn);
         double vx = qx - qn * ux, vy = qy - qn * uy, vz = qz - qn * uz;
         vxp[i] = (float)(-2.0 * k * vx);
         vyp[i] = (float)(-2.0 * k * vy);
         vzp[i] = (float)(-2.0 * k * vz);
-        q2p[i] = FAST ? (float)(0.5 / qn) : (float)(2.0 * qn);
+        if (FAST) {
+            // 1/(2|q|): f32 reciprocal seed, one FP64 Newton step (relative
+            // error ~1e-14 before the final rounding to f32).
+            const double d2 = 2.0 * qn;
+            const double y0 = (double)__frcp_rn((float)d2);
+            q2p[i] = (float)fma(y0, fma(-d2, y0, 1.0), y0);
+        } else {
+            q2p[i] = (float)(2.0 * qn);
+        }
         if (UNIFORM) {
             nqp[i] = (float)(2.0 * ((double)sv.unx * qx + (double)sv.uny * qy + (double)sv.unz * qz));
         } else {
@@ -500,9 +513,6 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
             qyp[i] = (float)qy;
             qzp[i] = (float)qz;
         }
-        // Base phase k|q| in turns, carried in double-double: k|q| reaches
-        // 1e12 rad at 30 keV and 20 m, where one FP64 rounding is 1e-4 rad.
-        float fr = (float)dd_turns(sv.kt, sv.kt_lo, qx, qy, qz);
         float sp, cp;
         sincospif(2.0f * fr, &sp, &cp);
         ws.ph[i][lane] = make_float2(-kt * sp, kt * cp);
@@ -527,10 +537,13 @@ __device__ __forceinline__ void flush_points(const PrSolve& sv, int t, int g, in
             ws.hi[i * 4 + c][lane] = 0.f;
             ws.lo[i * 4 + c][lane] = 0.f;
         }
-        base[0 * slots + s] += v[0] * phr - v[1] * phi;
-        base[1 * slots + s] += v[0] * phi + v[1] * phr;
-        base[2 * slots + s] += v[2] * phr - v[3] * phi;
-        base[3 * slots + s] += v[2] * phi + v[3] * phr;
+        // Each slot is updated by this one thread, in chunk order, so the
+        // sums are the same as with plain read-modify-writes; the atomic
+        // form only lets the warp go on without waiting for the loads.
+        atomicAdd(base + 0 * slots + s, v[0] * phr - v[1] * phi);
+        atomicAdd(base + 1 * slots + s, v[0] * phi + v[1] * phr);
+        atomicAdd(base + 2 * slots + s, v[2] * phr - v[3] * phi);
+        atomicAdd(base + 3 * slots + s, v[2] * phi + v[3] * phr);
     }
 }
 
