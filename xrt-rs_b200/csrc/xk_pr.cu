@@ -447,7 +447,7 @@ struct PackedState {
 // evaluated in double-double arithmetic (error-free products by FMA, TwoSum,
 // one Newton correction of the square root).
 __device__ __forceinline__ double dd_turns(double kt_hi, double kt_lo, double qx, double qy,
-                                           double qz, double* qn) {
+                                           double qz, double* qn, double* inv2q) {
     const double p0 = qx * qx, p1 = qy * qy, p2 = qz * qz;
     const double e0 = fma(qx, qx, -p0), e1 = fma(qy, qy, -p1), e2 = fma(qz, qz, -p2);
     double s1 = p0 + p1;
@@ -461,7 +461,14 @@ __device__ __forceinline__ double dd_turns(double kt_hi, double kt_lo, double qx
     lo -= hi - s2;
     const double r = sqrt(hi);
     *qn = r;
-    const double rl = (fma(-r, r, hi) + lo) / (2.0 * r);
+    // 1/(2r): f32 reciprocal seed and one FP64 Newton step (~1e-14 relative);
+    // it scales the square root's low-order correction and is the sweep's
+    // 1/(2|q|).
+    const double d2 = 2.0 * r;
+    const double y0 = (double)__frcp_rn((float)d2);
+    const double y = fma(y0, fma(-d2, y0, 1.0), y0);
+    *inv2q = y;
+    const double rl = (fma(-r, r, hi) + lo) * y;
     const double ph = kt_hi * r;
     const double pe = fma(kt_hi, r, -ph) + (kt_hi * rl + kt_lo * r);
     return (ph - rint(ph)) + pe;
@@ -491,21 +498,13 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
         // Base phase k|q| in turns, carried in double-double (k|q| reaches
         // 1e12 rad at 30 keV and 20 m, where one FP64 rounding is 1e-4 rad);
         // the same square root gives |q|.
-        double qn;
-        const float fr = (float)dd_turns(sv.kt, sv.kt_lo, qx, qy, qz, &qn);
+        double qn, inv2q;
+        const float fr = (float)dd_turns(sv.kt, sv.kt_lo, qx, qy, qz, &qn, &inv2q);
         double vx = qx - qn * ux, vy = qy - qn * uy, vz = qz - qn * uz;
         vxp[i] = (float)(-2.0 * k * vx);
         vyp[i] = (float)(-2.0 * k * vy);
         vzp[i] = (float)(-2.0 * k * vz);
-        if (FAST) {
-            // 1/(2|q|): f32 reciprocal seed, one FP64 Newton step (relative
-            // error ~1e-14 before the final rounding to f32).
-            const double d2 = 2.0 * qn;
-            const double y0 = (double)__frcp_rn((float)d2);
-            q2p[i] = (float)fma(y0, fma(-d2, y0, 1.0), y0);
-        } else {
-            q2p[i] = (float)(2.0 * qn);
-        }
+        q2p[i] = FAST ? (float)inv2q : (float)(2.0 * qn);
         if (UNIFORM) {
             nqp[i] = (float)(2.0 * ((double)sv.unx * qx + (double)sv.uny * qy + (double)sv.unz * qz));
         } else {
@@ -514,7 +513,8 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
             qzp[i] = (float)qz;
         }
         float sp, cp;
-        sincospif(2.0f * fr, &sp, &cp);
+        // |fr| <= 1/2 turn: the SFU sin/cos is accurate to ~5e-7 on [-pi, pi].
+        __sincosf(6.28318530717958647692f * fr, &sp, &cp);
         ws.ph[i][lane] = make_float2(-kt * sp, kt * cp);
     }
 }
@@ -560,7 +560,7 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
         double turns = -sv.kt * ur;
         float f = (float)(turns - rint(turns));
         float sn, cs;
-        sincospif(2.0f * f, &sn, &cs);
+        __sincosf(6.28318530717958647692f * f, &sn, &cs);
         float rxf = (float)r.rx, ryf = (float)r.ry, rzf = (float)r.rz;
         float w = (float)(-2.0 * ur);
         float4 a = make_float4(rxf, ryf, rzf, (float)(sv.k * perp2));
