@@ -594,10 +594,12 @@ xk::Status fresnel_host(xk_ctx* ctx, const double* rx, const double* rz, const d
     double max_amp = 0.0, max_rx = 0.0, max_rz = 0.0;
     const double ox = 0.5 * (sc->x_min + sc->x_max), oz = 0.5 * (sc->z_min + sc->z_max);
     for (size_t j = 0; j < n; ++j) {
-        max_amp = std::max(max_amp, std::hypot(er[j], ei[j]));
+        // An upper bound of |es_j| is all the f16 scaling needs.
+        max_amp = std::max(max_amp, std::max(std::fabs(er[j]), std::fabs(ei[j])));
         max_rx = std::max(max_rx, std::fabs(rx[j] - ox));
         max_rz = std::max(max_rz, std::fabs(rz[j] - oz));
     }
+    max_amp *= 1.4142135623730951;
     double* out = ctx->out_field.as<double>();
     xk::FresnelIn in{d, d + n, d + 2 * n, d + 3 * n, n, energy, dist,
                      sc->x_min, sc->x_max, sc->z_min, sc->z_max, nx, nz, max_amp, max_rx, max_rz,

@@ -48,18 +48,22 @@ class FresnelResult:
 
 def fresnel_propagate(ray_x, ray_z, ray_es, energy: float, dist: float, screen: FresnelScreen,
                       path="separable", ctx=None, return_stats=False):
-    """Propagate rays at (x, z) with complex amplitudes ``ray_es`` to the
-    screen at distance ``dist`` [mm]; ``energy`` in eV."""
+    """Propagate rays at (x, z) with complex amplitudes ``ray_es`` (a complex
+    array, or a (re, im) pair of float64 arrays) to the screen at distance
+    ``dist`` [mm]; ``energy`` in eV."""
     if path not in _FRESNEL_PATHS:
         raise ValueError(f"unknown path {path!r} (separable or f64)")
     code = _FRESNEL_PATHS[path]
     x, z = _f64(ray_x), _f64(ray_z)
-    es = np.ascontiguousarray(np.asarray(ray_es, dtype=np.complex128))
-    if not (len(x) == len(z) == len(es)):
+    if isinstance(ray_es, tuple) and len(ray_es) == 2:
+        er, ei = _f64(ray_es[0]), _f64(ray_es[1])  # (re, im) arrays, used in place
+    else:
+        es = np.asarray(ray_es, dtype=np.complex128)
+        er, ei = np.ascontiguousarray(es.real), np.ascontiguousarray(es.imag)
+    if not (len(x) == len(z) == len(er) == len(ei)):
         raise ValueError("array length mismatch: ray_x, ray_z and ray_es differ in length")
     if screen.nx < 0 or screen.nz < 0:
         raise ValueError("nx and nz must be non-negative")
-    er, ei = np.ascontiguousarray(es.real), np.ascontiguousarray(es.imag)
     nx, nz = int(screen.nx), int(screen.nz)
     m = nx * nz
     re = np.zeros(m, dtype=np.float64)
