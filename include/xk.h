@@ -144,7 +144,12 @@ const char* xk_route_reason(int reason);
  *   "phase_budget"   bound on the FP32 residual phase in rad (default 512)
  *   "sweep"          -1 automatic, 0 SFU reciprocal, 1 packed f32x2 sweep
  *   "groups"         ray ranges per screen tile, 0 = automatic
- *   "items_per_warp" target work items per resident warp (automatic groups) */
+ *   "items_per_warp" target work items per resident warp (automatic groups)
+ *   "f64_reduction"  XK_PATH_F64 only: 0 (default) evaluates sin/cos of each
+ *                    FP64 phase with the library functions, as the reference
+ *                    does; 1 first reduces the phase by 2 pi with an FMA-based
+ *                    Cody-Waite step (same phase value and 1e-10 parity, about
+ *                    twice the throughput at phases of 1e10-1e13 rad) */
 int xk_set_option(xk_ctx* ctx, const char* name, double value);
 
 typedef struct xk_tune_result {

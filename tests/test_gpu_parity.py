@@ -274,3 +274,19 @@ def test_autotune_keeps_results_and_restores_options(ctx, oracle):
     # apply=False left the context's defaults in force
     _, st = run(ctx, rays, pix, "f32pr")
     assert st["phase_bound_rad"] <= 512.0 + 1e-9
+
+
+def test_f64_reduction_option_keeps_parity(ctx, oracle):
+    """The FMA-based reduction of the FP64 phase (option "f64_reduction")
+    gives the same 1e-10 parity as the library sin/cos, at 1 m and at the far
+    end of the range (25 keV, 8 m)."""
+    rays, pix = synth.config0(seed=2)
+    far, fpix, _ = synth.config3(seed=0, count=2, ray_range=(300, 30000), pix_range=(17, 4000))[1]
+    ctx.set_option("f64_reduction", 1)
+    try:
+        for r, p in ((rays, pix), (far, fpix)):
+            out, st = run(ctx, r, p, "f64")
+            assert st["path"] == xrt_rs.XK_PATH_F64
+            assert cases.rel_l2(out, oracle_run(oracle, r, p)) < F64_TOL
+    finally:
+        ctx.set_option("f64_reduction", 0)

@@ -320,6 +320,9 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
     } else if (n == "groups") {
         if (value < 0.0 || value > 65536.0) return fail(ctx, XK_ERR_INVALID, "groups out of range");
         ctx->pr_opts.groups = (int)value;
+    } else if (n == "f64_reduction") {
+        if (value != 0.0 && value != 1.0) return fail(ctx, XK_ERR_INVALID, "f64_reduction is 0 or 1");
+        ctx->f64ws.fast_reduction = value != 0.0;
     } else if (n == "items_per_warp") {
         if (value < 1.0 || value > 4096.0) return fail(ctx, XK_ERR_INVALID, "items_per_warp out of range");
         ctx->pr_opts.items_per_warp = (long long)value;

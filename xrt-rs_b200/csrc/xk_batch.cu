@@ -110,6 +110,7 @@ xk::Status create_batch(xk_ctx* ctx, const xk_solve* solves, size_t n, int path,
     b->inputs.async_stream = b->stream;
     b->f64ws.rays.async_stream = b->stream;
     b->f64ws.partials.async_stream = b->stream;
+    b->f64ws.fast_reduction = ctx->f64ws.fast_reduction;
     const bool device = (flags & XK_BATCH_DEVICE) != 0;
 
     // Device views of every solve; host inputs are copied once into one buffer.

@@ -67,6 +67,27 @@ __device__ __forceinline__ void kahan_add(double& sum, double& comp, double term
     sum = t;
 }
 
+// sin and cos of a large FP64 phase x (|x| < 2^52; here k|p - r| <= ~1e13):
+// Cody-Waite reduction by 2*pi written with FMAs. 2*pi is split into three
+// doubles T1 = fl(2 pi), T2 = fl(2 pi - T1), T3 = fl(2 pi - T1 - T2) (from
+// Machin's formula to 80 digits); n = rint(x / 2 pi), n*T1 is formed exactly
+// as a rounded product plus its FMA error term, x - n*T1 is exact (Sterbenz),
+// and the remaining terms leave r = x - 2 pi n with an absolute error of a few
+// 1e-16 for every phase this path meets. sin/cos of |r| <= pi then take the
+// short path of the library functions.
+__device__ __forceinline__ void sincos_large(double x, double* s, double* c) {
+    constexpr double kT1 = 6.283185307179586, kT2 = 2.4492935982947064e-16,
+                     kT3 = -5.989539619436679e-33, kInv = 0.15915494309189535;
+    const double n = rint(x * kInv);
+    const double p1 = n * kT1;
+    const double e1 = fma(n, kT1, -p1);
+    double r = (x - p1) - e1;
+    r = fma(-n, kT2, r);
+    r = fma(-n, kT3, r);
+    sincos(r, s, c);
+}
+
+template <bool REDUCE>
 __device__ __forceinline__ void pair_f64(const RayRec64& r, double px, double py, double pz,
                                          Acc& a) {
     double dx = __dsub_rn(px, r.x);
@@ -79,7 +100,8 @@ __device__ __forceinline__ void pair_f64(const RayRec64& r, double px, double py
     double ns = __ddiv_rn(nd, path);
     double phase = __dmul_rn(r.k, path);
     double s, c;
-    sincos(phase, &s, &c);
+    if (REDUCE) sincos_large(phase, &s, &c);
+    else sincos(phase, &s, &c);
     double obl = __dadd_rn(r.nl, ns);
     double af = __ddiv_rn(__dmul_rn(r.kf, obl), path);
     // u = i*af*exp(i*phase) = (-af*sin, af*cos)  (diffraction.rs:98)
@@ -95,6 +117,7 @@ __device__ __forceinline__ void pair_f64(const RayRec64& r, double px, double py
     kahan_add(a.s[3], a.c[3], ti);
 }
 
+template <bool REDUCE>
 __global__ void __launch_bounds__(kF64Threads)
 f64_pairs_kernel(const RayRec64* __restrict__ rays, size_t n_rays, size_t rays_per_split,
                  PixDev pix, size_t n_pix, FieldDev out, double* __restrict__ partials) {
@@ -127,7 +150,7 @@ f64_pairs_kernel(const RayRec64* __restrict__ rays, size_t n_rays, size_t rays_p
         __syncthreads();
         for (int j = 0; j < cnt; ++j) {
 #pragma unroll
-            for (int i = 0; i < kF64Ppt; ++i) pair_f64(sm[j], px[i], py[i], pz[i], acc[i]);
+            for (int i = 0; i < kF64Ppt; ++i) pair_f64<REDUCE>(sm[j], px[i], py[i], pz[i], acc[i]);
         }
     }
 
@@ -227,8 +250,12 @@ Status f64_enqueue(const RaysDev& rays, size_t n_rays, const PixDev& pix, size_t
         partials = ws.partials.as<double>();
     }
     dim3 grid((unsigned)pix_ctas, (unsigned)splits);
-    f64_pairs_kernel<<<grid, kF64Threads, 0, stream>>>(packed, n_rays, rays_per_split, pix, n_pix,
-                                                         out, partials);
+    if (ws.fast_reduction)
+        f64_pairs_kernel<true><<<grid, kF64Threads, 0, stream>>>(packed, n_rays, rays_per_split,
+                                                                 pix, n_pix, out, partials);
+    else
+        f64_pairs_kernel<false><<<grid, kF64Threads, 0, stream>>>(packed, n_rays, rays_per_split,
+                                                                  pix, n_pix, out, partials);
     XK_CUDA_TRY(cudaGetLastError());
     int kernels = 2;
     if (splits > 1) {
@@ -347,8 +374,8 @@ extern "C" int xk_diffraction_f64_noalloc(const xk_rays* rays, size_t n_rays,
     f64_pack_kernel<<<(unsigned)((n_rays + 255) / 256), 256, 0, s>>>(rd, n_rays, packed);
     if (cudaGetLastError() != cudaSuccess) return XK_ERR_CUDA;
     dim3 grid((unsigned)pix_ctas, (unsigned)splits);
-    f64_pairs_kernel<<<grid, kF64Threads, 0, s>>>(packed, n_rays, rays_per_split, pd, n_pix, fd,
-                                                   partials);
+    f64_pairs_kernel<false><<<grid, kF64Threads, 0, s>>>(packed, n_rays, rays_per_split, pd,
+                                                          n_pix, fd, partials);
     if (cudaGetLastError() != cudaSuccess) return XK_ERR_CUDA;
     if (splits > 1) {
         f64_combine_kernel<<<(unsigned)((n_pix + 255) / 256), 256, 0, s>>>(partials, (int)splits,

@@ -113,6 +113,10 @@ struct FieldDev {
 struct F64Workspace {
     DevBuf rays;      // packed ray records
     DevBuf partials;  // split-ray partial sums
+    // false: sin/cos of each phase k|p - r| by the library functions, as the
+    // reference computes them; true: an FMA-based reduction by 2 pi first
+    // (same phase, same parity bar, about twice as fast at 1e10-1e13 rad).
+    bool fast_reduction = false;
 };
 
 struct LaunchReport {

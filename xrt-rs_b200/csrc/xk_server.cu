@@ -640,6 +640,7 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
     XK_TRY(xk::pr_reserve_plan_host(s->plan_ws, kPlanBatch, s->num_sms));
     s->f64ws.rays.async_stream = s->f64_stream;
     s->f64ws.partials.async_stream = s->f64_stream;
+    s->f64ws.fast_reduction = ctx->f64ws.fast_reduction;
     s->worker = std::thread(worker_loop, s);
     s->planner = std::thread(planner_loop, s);
     s->finisher = std::thread(finisher_loop, s);
