@@ -320,6 +320,67 @@ __global__ void records_kernel(RaysDev r, int n, const int* __restrict__ sorted_
     recs[i] = rec;
 }
 
+// Orders the ray groups of a solve by decreasing estimated cost, so that the
+// persistent kernel hands out the most expensive (tile, group) items first and
+// the launch does not end on a few long ones. A group's cost is its ray count
+// plus kGroupChunkCost rays for every chunk it spans (each chunk boundary
+// costs a per-point set-up and flush, about the sweep of that many rays).
+// One block, bitonic sort of (cost, group) keys in shared memory; ties keep
+// group order, so the schedule is deterministic. groups <= kMaxGroups.
+constexpr int kMaxGroups = 4096;
+constexpr int kGroupChunkCost = 24;
+
+__global__ void __launch_bounds__(1024) group_order_kernel(const int* __restrict__ chunk_begin,
+                                                           const int* __restrict__ n_chunks_dev,
+                                                           int n, int groups,
+                                                           int* __restrict__ order) {
+    __shared__ unsigned long long key[kMaxGroups];
+    const int n_chunks = *n_chunks_dev;
+    int len = 1;
+    while (len < groups) len <<= 1;
+    auto chunk_at = [&](int pos) {
+        int lo = 0, hi = n_chunks - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (chunk_begin[mid] <= pos) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    };
+    for (int g = threadIdx.x; g < len; g += blockDim.x) {
+        unsigned long long k = ~0ull;
+        if (g < groups) {
+            const long long r0 = (long long)g * n / groups, r1 = (long long)(g + 1) * n / groups;
+            unsigned int cost = 0;
+            if (r1 > r0) {
+                const int c = chunk_at((int)(r1 - 1)) - chunk_at((int)r0) + 1;
+                const long long w = (r1 - r0) + (long long)kGroupChunkCost * c;
+                cost = (unsigned int)(w < 0x7fffffffLL ? w : 0x7fffffffLL);
+            }
+            // Ascending keys = descending cost, then ascending group.
+            k = ((unsigned long long)(0xffffffffu - cost) << 32) | (unsigned int)g;
+        }
+        key[g] = k;
+    }
+    __syncthreads();
+    for (int size = 2; size <= len; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < len; i += blockDim.x) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const unsigned long long a = key[i], b = key[j];
+                    if ((a > b) == up) {
+                        key[i] = b;
+                        key[j] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < groups; i += blockDim.x) order[i] = (int)(key[i] & 0xffffffffu);
+}
+
 // Adds the groups' slots of every tile slot in order and scatters the sum to
 // the screen point's original index.
 __global__ void finalize_kernel(const double* __restrict__ partial, const int* __restrict__ tile_perm,
@@ -748,7 +809,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
     // groups * n_tiles consecutive items of a solve).
     const int t = (int)(local % sv.n_tiles);
     const long long rest = local / sv.n_tiles;
-    const int g = (int)(rest % sv.groups);
+    const int g = sv.group_order[(int)(rest % sv.groups)];
     const int sub = (int)(rest / sv.groups);
     const long long n = sv.n_rays;
     const long long g0 = (long long)g * n / sv.groups;
@@ -964,6 +1025,7 @@ struct SolveBufs {
     int* chunk_begin;
     double* chunk_center;
     int* n_chunks;
+    int* group_order;
     PrRawRay* recs;
     double* partial;
 };
@@ -990,6 +1052,7 @@ void carve(Arena& a, SolveBufs& b, int n, int m, int n_tiles, int groups, int su
     b.chunk_begin = a.take<int>((size_t)n + 1);
     b.chunk_center = a.take<double>(3 * (size_t)n);
     b.n_chunks = a.take<int>(1);
+    b.group_order = a.take<int>(groups);
     b.recs = a.take<PrRawRay>(n);
     b.partial = a.take<double>((size_t)groups * 4 * slots);
 }
@@ -1028,13 +1091,13 @@ int sum_blocks_for(int num_sms) { return std::min(512, std::max(1, 2 * num_sms))
 // Ray groups per tile: enough items to keep every resident warp busy, at
 // least four stages of rays per item, partial slots within 1 GiB.
 int plan_groups(int n, int n_tiles, int num_sms, const PrOptions& opt) {
-    if (opt.groups > 0) return opt.groups;
+    if (opt.groups > 0) return std::min(opt.groups, kMaxGroups);
     long long want = (long long)num_sms * 12 * opt.items_per_warp;
     int g = (int)std::max<long long>(1, (want + n_tiles - 1) / n_tiles);
     g = std::min(g, std::max(1, n / (4 * kPrStage)));
     long long cap = (1LL << 30) / (32LL * n_tiles * kPrTile);
     g = (int)std::max<long long>(1, std::min<long long>(g, cap));
-    return std::min(g, 4096);
+    return std::min(g, kMaxGroups);
 }
 
 }  // namespace
@@ -1355,7 +1418,10 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         records_kernel<<<(n + 255) / 256, 256, 0, stream>>>(in[s].rays, n, B.ri_out, B.run,
                                                              B.chunk_center, B.recs);
         XK_CUDA_TRY(cudaGetLastError());
-        nk += 5;
+        group_order_kernel<<<1, 1024, 0, stream>>>(B.chunk_begin, B.n_chunks, n, groups[s],
+                                                   B.group_order);
+        XK_CUDA_TRY(cudaGetLastError());
+        nk += 6;
 
         PrSolve& D = P.dev;
         D.recs = B.recs;
@@ -1366,6 +1432,7 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         D.tpy = B.tpy;
         D.tpz = B.tpz;
         D.tile_center = B.tile_center;
+        D.group_order = B.group_order;
         D.partial = B.partial;
         D.item_begin = 0;
         D.item_offset = 0;

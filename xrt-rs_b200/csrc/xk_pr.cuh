@@ -45,6 +45,7 @@ struct PrSolve {
     const int* n_chunks_dev;      // scalar
     const double *tpx, *tpy, *tpz;  // screen points in tile-slot order (padding = tile centre)
     const double* tile_center;    // [3 * n_tiles]
+    const int* group_order;       // [groups] ray groups by decreasing estimated cost
     double* partial;              // [groups][4][n_tiles * kPrTile], tile-slot order
     long long item_begin;         // first global item of this solve in its launch
     long long item_offset;        // first of the solve's own items covered by the launch
