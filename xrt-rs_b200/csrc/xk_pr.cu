@@ -59,6 +59,8 @@ constexpr uint32_t kMaxWaitIters = 1u << 24;
 constexpr int kFoldStages = 1;
 // |e| bound under which the packed sweep's series reciprocal is used.
 constexpr double kSeriesRcpBound = 2e-3;
+// Fold the base phase when the estimated chunks per ray group reach this.
+constexpr double kFoldChunksPerGroup = 4.0;
 
 // ---------------------------------------------------------------------------
 // Planner kernels
@@ -480,7 +482,7 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 struct WarpShared {
     float hi[kPrPpl * 4][32];  // two-float accumulators, [point*4 + component][lane]
     float lo[kPrPpl * 4][32];
-    float2 ph[kPrPpl][32];     // (k/2pi) i exp(i k |q|) of the current chunk
+    float2 ph[kPrPpl][32];     // (k/2pi) i exp(i k |q|) of the current chunk (unfolded variants)
     double ux, uy, uz;         // item direction for the current chunk
     double r0x, r0y, r0z;      // chunk centre
     uint64_t bar[2];           // mbarriers of the two ray buffers
@@ -492,6 +494,7 @@ struct ScalarState {
     float vx[kPrPpl], vy[kPrPpl], vz[kPrPpl], q2[kPrPpl];  // q2 = 2|q|
     float nq[kPrPpl];                                        // 2 n.q (UNIFORM)
     float qx[kPrPpl], qy[kPrPpl], qz[kPrPpl];                // q (general normals)
+    float phi[kPrPpl];                                       // base phase k|q| mod 2 pi
     float acc[kPrPpl][4];
 };
 
@@ -501,6 +504,7 @@ struct PackedState {
     float2 vx[kPrPpl / 2], vy[kPrPpl / 2], vz[kPrPpl / 2], q2[kPrPpl / 2];  // q2 = 1/(2|q|)
     float2 nq[kPrPpl / 2];
     float2 qx[kPrPpl / 2], qy[kPrPpl / 2], qz[kPrPpl / 2];
+    float2 phi[kPrPpl / 2];  // base phase k|q| mod 2 pi
     float2 acc[kPrPpl / 2][4];
 };
 
@@ -536,14 +540,14 @@ __device__ __forceinline__ double dd_turns(double kt_hi, double kt_lo, double qx
 }
 
 // Per chunk: FP64 geometry of the lane's points, written into the sweep
-// state, and the per-point phasor into shared memory.
-template <bool UNIFORM, bool FAST, class State>
+// state, and the per-point base phase k|q|: folded into the sweep state
+// (FOLD) or as the chunk phasor (k/2pi) i exp(i k|q|) into shared memory.
+template <bool UNIFORM, bool FAST, bool FOLD, class State>
 __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane, WarpShared& ws,
                                              State& st) {
     const double ux = ws.ux, uy = ws.uy, uz = ws.uz;
     const double r0x = ws.r0x, r0y = ws.r0y, r0z = ws.r0z;
     const double k = sv.k;
-    const float kt = (float)sv.kt;
     float* vxp = reinterpret_cast<float*>(st.vx);
     float* vyp = reinterpret_cast<float*>(st.vy);
     float* vzp = reinterpret_cast<float*>(st.vz);
@@ -573,17 +577,25 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
             qyp[i] = (float)qy;
             qzp[i] = (float)qz;
         }
-        float sp, cp;
-        // |fr| <= 1/2 turn: the SFU sin/cos is accurate to ~5e-7 on [-pi, pi].
-        __sincosf(6.28318530717958647692f * fr, &sp, &cp);
-        ws.ph[i][lane] = make_float2(-kt * sp, kt * cp);
+        if (FOLD) {
+            // The base phase enters the FP32 residual phase of every pair of
+            // the chunk (|fr| <= 1/2 turn), so the chunk sums need no phasor.
+            reinterpret_cast<float*>(st.phi)[i] = 6.28318530717958647692f * fr;
+        } else {
+            // |fr| <= 1/2 turn: the SFU sin/cos is accurate to ~5e-7 on [-pi, pi].
+            const float kt = (float)sv.kt;
+            float sp, cp;
+            __sincosf(6.28318530717958647692f * fr, &sp, &cp);
+            ws.ph[i][lane] = make_float2(-kt * sp, kt * cp);
+        }
     }
 }
 
-// Multiplies the lane's two-float sums by the chunk phasor in FP64 and adds
-// them to the item's slots (tile-slot order), then clears the sums.
-__device__ __forceinline__ void flush_points(const PrSolve& sv, int t, int g, int lane,
-                                             WarpShared& ws) {
+// Unfolded variants, at every chunk boundary and at the item end: multiplies
+// the lane's two-float chunk sums by the chunk phasor in FP64, adds them to
+// the item's slots (tile-slot order) and clears the sums.
+__device__ __forceinline__ void flush_chunk(const PrSolve& sv, int t, int g, int lane,
+                                            WarpShared& ws) {
     const size_t slots = (size_t)sv.n_tiles * kPrTile;
     double* base = sv.partial + (size_t)g * 4 * slots;
 #pragma unroll 2
@@ -598,13 +610,36 @@ __device__ __forceinline__ void flush_points(const PrSolve& sv, int t, int g, in
             ws.hi[i * 4 + c][lane] = 0.f;
             ws.lo[i * 4 + c][lane] = 0.f;
         }
-        // Each slot is updated by this one thread, in chunk order, so the
-        // sums are the same as with plain read-modify-writes; the atomic
+        // Each slot is updated by this one thread, in chunk order; the atomic
         // form only lets the warp go on without waiting for the loads.
         atomicAdd(base + 0 * slots + s, v[0] * phr - v[1] * phi);
         atomicAdd(base + 1 * slots + s, v[0] * phi + v[1] * phr);
         atomicAdd(base + 2 * slots + s, v[2] * phr - v[3] * phi);
         atomicAdd(base + 3 * slots + s, v[2] * phi + v[3] * phr);
+    }
+}
+
+// Folded variants, once at the item end: multiplies the lane's two-float
+// sums of the item by i k / (2 pi) in FP64 and adds them to the item's slots.
+__device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int lane,
+                                             WarpShared& ws) {
+    const size_t slots = (size_t)sv.n_tiles * kPrTile;
+    double* base = sv.partial + (size_t)g * 4 * slots;
+    const double kt = sv.kt;
+#pragma unroll 2
+    for (int i = 0; i < kPrPpl; ++i) {
+        const size_t s = (size_t)t * kPrTile + lane + 32 * i;
+        double v[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            v[c] = (double)ws.hi[i * 4 + c][lane] + (double)ws.lo[i * 4 + c][lane];
+        // Sub-items of one (group, tile) add into the same slots in sub
+        // order (never two in one launch); the atomic form only lets the warp
+        // go on without waiting for the loads.
+        atomicAdd(base + 0 * slots + s, -kt * v[1]);
+        atomicAdd(base + 1 * slots + s, kt * v[0]);
+        atomicAdd(base + 2 * slots + s, -kt * v[3]);
+        atomicAdd(base + 3 * slots + s, kt * v[2]);
     }
 }
 
@@ -689,7 +724,7 @@ __device__ __forceinline__ void clear_acc(PackedState<UNIFORM>& ls) {
 }
 
 // SFU sweep: one point per FP32 instruction, rcp.approx for the reciprocal.
-template <bool UNIFORM>
+template <bool UNIFORM, bool FOLD>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
                                             ScalarState<UNIFORM>& ls, WarpShared& ws) {
     const float4* rec = reinterpret_cast<const float4*>(buf);
@@ -706,7 +741,7 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             num = fmaf(ls.vy[i], a.y, num);
             num = fmaf(ls.vz[i], a.z, num);
             const float rd = rcp_approx(ls.q2[i] + b.x);
-            const float th = num * rd;
+            const float th = FOLD ? fmaf(num, rd, ls.phi[i]) : num * rd;
             float sn, cs;
             __sincosf(th, &sn, &cs);
             float gq;
@@ -727,7 +762,7 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
 }
 
 // Packed sweep: two points per f32x2 instruction, series reciprocal.
-template <bool UNIFORM>
+template <bool UNIFORM, bool FOLD>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
                                             PackedState<UNIFORM>& ls, WarpShared& ws) {
     constexpr int H = kPrPpl / 2;
@@ -751,7 +786,7 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             // 1/(2|q| - 2u.rho) = r0 / (1 - e), e = 2u.rho r0 ~ r0 (1 + e + e^2)
             const float2 ep = __fmul2_rn(wn, ls.q2[i]);
             const float2 rd = __ffma2_rn(ls.q2[i], __ffma2_rn(ep, ep, ep), ls.q2[i]);
-            const float2 th = __fmul2_rn(num, rd);
+            const float2 th = FOLD ? __ffma2_rn(num, rd, ls.phi[i]) : __fmul2_rn(num, rd);
             float s0, c0, s1, c1;
             __sincosf(th.x, &s0, &c0);
             __sincosf(th.y, &s1, &c1);
@@ -800,7 +835,7 @@ __device__ __forceinline__ int chunk_of(const int* __restrict__ begin, int n_chu
 }
 
 // Processes one (tile, ray-range) item; false if a bounded wait ran out.
-template <bool UNIFORM, bool FAST>
+template <bool UNIFORM, bool FAST, bool FOLD>
 __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, WarpShared& ws,
                              int lane) {
     // local = (sub * groups + g) * n_tiles + t: sub-range `sub` of ray group g
@@ -854,7 +889,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
             return false;
         }
         if (c != cur_chunk) {
-            if (cur_chunk >= 0) flush_points(sv, t, g, lane, ws);
+            if (!FOLD && cur_chunk >= 0) flush_chunk(sv, t, g, lane, ws);
             __syncwarp();
             if (lane == 0) {
                 const double p0x = sv.tile_center[3 * t], p0y = sv.tile_center[3 * t + 1],
@@ -871,12 +906,12 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
                 ws.r0z = r0z;
             }
             __syncwarp();
-            setup_points<UNIFORM, FAST>(sv, t, lane, ws, st);
+            setup_points<UNIFORM, FAST, FOLD>(sv, t, lane, ws, st);
             cur_chunk = c;
         }
         prep_stage(wp.buf[b], len, lane, sv, ws);
         __syncwarp();
-        sweep_stage<UNIFORM>(wp.buf[b], len, lane, st, ws);
+        sweep_stage<UNIFORM, FOLD>(wp.buf[b], len, lane, st, ws);
         // FP32 partials run over at most kFoldStages stages of one chunk.
         if (++since_fold == kFoldStages || nlen == 0 || nc != c) {
             fold_acc(st, ws, lane);
@@ -892,7 +927,8 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
         len = nlen;
         b ^= 1;
     }
-    flush_points(sv, t, g, lane, ws);
+    if (FOLD) flush_item(sv, t, g, lane, ws);
+    else flush_chunk(sv, t, g, lane, ws);
     __syncwarp();
     return true;
 }
@@ -901,7 +937,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
 // sweep); solves[s].item_begin is the prefix sum of the item counts in this
 // launch, and the launch covers items [item_offset, item_offset + count) of
 // each solve.
-template <bool UNIFORM, bool FAST>
+template <bool UNIFORM, bool FAST, bool FOLD>
 __global__ void __launch_bounds__(kPrWarpsPerCta * 32, 3)
 pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long n_items,
                      unsigned long long* __restrict__ counter, int* __restrict__ err) {
@@ -936,7 +972,7 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
         }
         const PrSolve& sv = solves[lo];
         const long long local = item - sv.item_begin + sv.item_offset;
-        const bool ok = process_item<UNIFORM, FAST>(sv, local, wp, *wsh, lane);
+        const bool ok = process_item<UNIFORM, FAST, FOLD>(sv, local, wp, *wsh, lane);
         if (!ok) {
             if (lane == 0) atomicExch(err, 1);
             break;
@@ -949,9 +985,15 @@ constexpr size_t kPrSmemBytes = (size_t)kPrWarpsPerCta * 2 * kPrStage * sizeof(P
 
 using PrKernel = void (*)(const PrSolve*, int, long long, unsigned long long*, int*);
 
-PrKernel pr_kernel(bool uniform, bool fast) {
-    if (uniform) return fast ? pr_persistent_kernel<true, true> : pr_persistent_kernel<true, false>;
-    return fast ? pr_persistent_kernel<false, true> : pr_persistent_kernel<false, false>;
+// Kernel of a variant: bit 0 uniform normal, bit 1 packed sweep, bit 2 folded
+// base phase (PrPlan::variant()).
+PrKernel pr_kernel(int variant) {
+    static const PrKernel table[8] = {
+        pr_persistent_kernel<false, false, false>, pr_persistent_kernel<true, false, false>,
+        pr_persistent_kernel<false, true, false>,  pr_persistent_kernel<true, true, false>,
+        pr_persistent_kernel<false, false, true>,  pr_persistent_kernel<true, false, true>,
+        pr_persistent_kernel<false, true, true>,   pr_persistent_kernel<true, true, true>};
+    return table[variant & 7];
 }
 
 // ---------------------------------------------------------------------------
@@ -1401,6 +1443,16 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         // argument.
         P.rcp_bound = b_max / std::max(I.d_lo - b_max, 1e-300);
         P.fast = opt.sweep == 1 || (opt.sweep < 0 && P.rcp_bound <= kSeriesRcpBound);
+        {
+            // Fold the base phase into the sweep when ray groups span many
+            // chunks (near field): per-chunk flushes then disappear, at the
+            // price of a three-operand phase FMA per pair (about 1.4 % of the
+            // sweep). Non-empty cells bound the chunk count from above.
+            double cells = 1.0;
+            for (int ax = 0; ax < 3; ++ax) cells *= (double)cg.n[ax];
+            const double est_chunks = std::min(cells, (double)n);
+            P.fold = est_chunks >= kFoldChunksPerGroup * (double)groups[s];
+        }
 
         ray_keys_kernel<<<(n + 255) / 256, 256, 0, stream>>>(in[s].rays, n, cg, B.rk_in, B.ri_in);
         XK_CUDA_TRY(cudaGetLastError());
@@ -1469,11 +1521,11 @@ Status pr_zero_partials(const PrPlan& P, cudaStream_t stream) {
     return Status::Ok();
 }
 
-Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, bool uniform, bool fast,
+Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int variant,
                  unsigned long long* d_counter, int* d_err, cudaStream_t stream, int num_sms,
                  int max_ctas_per_sm) {
     if (n_items <= 0) return Status::Ok();
-    PrKernel kern = pr_kernel(uniform, fast);
+    PrKernel kern = pr_kernel(variant);
     XK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)kPrSmemBytes));
     int per_sm = 0;
@@ -1531,16 +1583,15 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
     struct Launch {
         int first, count;
         long long items;
-        bool uniform, fast;
+        int variant;
     };
     std::vector<Launch> launches;
     int tab = 0;
-    for (int variant = 0; variant < 4; ++variant) {
-        const bool uniform = (variant & 1) != 0, fast = (variant & 2) != 0;
-        Launch L{tab, 0, 0, uniform, fast};
+    for (int variant = 0; variant < kPrVariants; ++variant) {
+        Launch L{tab, 0, 0, variant};
         for (int s = 0; s < count; ++s) {
             PrPlan& P = plans[s];
-            if (P.routed || P.uniform_normal != uniform || P.fast != fast) continue;
+            if (P.routed || P.variant() != variant) continue;
             P.dev.item_begin = L.items;
             h_tab[tab++] = P.dev;
             L.items += P.dev.n_items;
@@ -1556,7 +1607,7 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
     int li = 0;
     for (const Launch& L : launches) {
         XK_TRY(pr_launch(reinterpret_cast<const PrSolve*>(ws.solves.ptr) + L.first, L.count,
-                         L.items, L.uniform, L.fast, d_counters + li, d_err, stream, num_sms, 0));
+                         L.items, L.variant, d_counters + li, d_err, stream, num_sms, 0));
         R.kernels += 1;
         R.n_items += L.items;
         ++li;

@@ -73,6 +73,9 @@ struct PrPlan {
     int route_reason = 0;
     bool uniform_normal = false;
     bool fast = false;  // packed sweep with Newton reciprocal
+    bool fold = false;  // base phase folded into the per-pair phase (near field)
+    // Kernel variant: bit 0 uniform normal, bit 1 packed sweep, bit 2 folded.
+    int variant() const { return (uniform_normal ? 1 : 0) | (fast ? 2 : 0) | (fold ? 4 : 0); }
     int n_tiles = 0, groups = 0, n_chunks = 0;
     double phase_bound = 0.0, rcp_bound = 0.0;
     PrSolve dev{};
@@ -135,7 +138,8 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
 // clear a plan's partial slots; one persistent launch over a device table of
 // solves (all of one variant) covering n_items items; a plan's final reduction.
 Status pr_zero_partials(const PrPlan& P, cudaStream_t stream);
-Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, bool uniform, bool fast,
+constexpr int kPrVariants = 8;
+Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int variant,
                  unsigned long long* d_counter, int* d_err, cudaStream_t stream, int num_sms,
                  int max_ctas_per_sm);
 Status pr_finalize(const PrPlan& P, cudaStream_t stream);

@@ -79,7 +79,7 @@ struct Req {
 };
 
 constexpr int kEpochRing = 3;
-constexpr int kVariants = 4;
+constexpr int kVariants = xk::kPrVariants;
 constexpr int kPlanBatch = 32;  // requests planned together at most
 
 struct EpochSlot {
@@ -352,14 +352,13 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
 
     // One table, grouped by kernel variant.
     int tab = 0;
-    long long counts[kVariants] = {0, 0, 0, 0};
-    int first[kVariants] = {0, 0, 0, 0}, nsol[kVariants] = {0, 0, 0, 0};
+    long long counts[kVariants] = {};
+    int first[kVariants] = {}, nsol[kVariants] = {};
     for (int v = 0; v < kVariants; ++v) {
-        const bool uniform = (v & 1) != 0, fast = (v & 2) != 0;
         first[v] = tab;
         for (const Take& t : takes) {
             const xk::PrPlan& P = t.q->plan;
-            if (P.uniform_normal != uniform || P.fast != fast) continue;
+            if (P.variant() != v) continue;
             xk::PrSolve d = P.dev;
             d.item_begin = counts[v];
             d.item_offset = t.first;
@@ -376,8 +375,8 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
     const int sms = std::max(1, s->num_sms - std::max(0, s->opts.reserve_sms));
     for (int v = 0; v < kVariants; ++v) {
         if (!nsol[v]) continue;
-        XK_TRY(xk::pr_launch(e.table.as<xk::PrSolve>() + first[v], nsol[v], counts[v], (v & 1) != 0,
-                             (v & 2) != 0, counters + v, d_err, s->exec_stream, sms, 0));
+        XK_TRY(xk::pr_launch(e.table.as<xk::PrSolve>() + first[v], nsol[v], counts[v], v,
+                             counters + v, d_err, s->exec_stream, sms, 0));
         s->kernels++;
     }
     XK_CUDA_TRY(cudaMemcpyAsync(e.h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s->exec_stream));
