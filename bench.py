@@ -74,6 +74,12 @@ def parse():
     ap.add_argument("--sweep-sample", type=int, default=64,
                     help="screen points per cell checked against the CPU oracle")
     ap.add_argument("--batch-count", type=int, default=64)
+    ap.add_argument("--epoch-pairs", type=float, default=0.0,
+                    help="serve: pairs per epoch (0 = the server's default)")
+    ap.add_argument("--item-pairs", type=float, default=0.0,
+                    help="serve: pairs per work item (0 = the server's default)")
+    ap.add_argument("--reserve-sms", type=int, default=0,
+                    help="serve: SMs left to planning (0 = the server's default)")
     return ap.parse_args()
 
 
@@ -462,7 +468,8 @@ def run_serve(args):
     ctx = xrt_rs.GpuContext.new(0)
     reqs = synth.config4_requests(seed=0, rate_hz=args.rate, duration_s=args.duration)
     base = synth.gaussian_aperture(2_000_000, 0.1, 10_000.0, 30_000.0, seed=1)
-    srv = Server(ctx, hbm_budget_bytes=120e9)
+    srv = Server(ctx, hbm_budget_bytes=120e9, epoch_pairs=args.epoch_pairs,
+                 item_pairs=args.item_pairs, reserve_sms=args.reserve_sms)
     sets = {}
     lat, done_pairs, failures = [], [0.0], [0]
     lock = threading.Lock()
@@ -536,6 +543,7 @@ def run_serve(args):
             pending.append((t, float(n) * len(screen["x"])))
         submitted += 1
     window = time.perf_counter() - t0
+    launched_in_window = srv.stats()["pairs_launched"]
     stop.set()
     for w in waiters:
         w.join(timeout=args.drain + 30)
@@ -551,6 +559,9 @@ def run_serve(args):
         "p50_ms": float(np.percentile(lat_a, 50)), "p90_ms": float(np.percentile(lat_a, 90)),
         "p99_ms": float(np.percentile(lat_a, 99)),
         "gpair_s_served": done_pairs[0] / elapsed / 1e9,
+        # Pairs of all work items launched during the arrival window (partly
+        # served requests included): the device throughput under this load.
+        "gpair_s_launched_in_window": launched_in_window / window / 1e9,
         "offered_gpair_s": sum(r["n_rays"] * max(16, int(round(np.sqrt(r["n_pix"])))) ** 2
                                for r in reqs) / args.duration / 1e9,
         "epochs": st["epochs"], "peak_bytes": st["peak_bytes"], "hbm_budget_bytes": 120e9,

@@ -356,9 +356,9 @@ typedef struct xk_server xk_server;
 
 typedef struct xk_server_opts {
     double hbm_budget_bytes;          /* admission budget; 0 = 120e9 */
-    double epoch_pairs;               /* ray x screen pairs per epoch; 0 = 2e10 */
+    double epoch_pairs;               /* ray x screen pairs per epoch; 0 = 3e10 */
     int max_active;                   /* admitted requests at once; 0 = 64 */
-    double item_pairs;                /* target pairs per work item; 0 = 4e6 */
+    double item_pairs;                /* target pairs per work item; 0 = 1e6 */
     int inject_alloc_failure_every;   /* testing: fail every k-th request allocation; 0 = off */
     int reserve_sms;                  /* SMs epochs leave free for planning kernels; 0 = 8 */
 } xk_server_opts;
@@ -387,6 +387,7 @@ typedef struct xk_request_stats {
 typedef struct xk_server_stats {
     long long submitted, completed, failed, epochs, kernels, pending, active;
     double pairs_done, used_bytes, peak_bytes, resident_ray_bytes;
+    double pairs_launched;  /* ray x screen pairs of all work items launched so far */
 } xk_server_stats;
 
 int xk_server_create(xk_ctx* ctx, const xk_server_opts* opts, xk_server** out);

@@ -32,8 +32,6 @@
 //   accumulators so that draining overlaps the next segment. K-split partials
 //   are added in FP64 in split order (results do not depend on scheduling).
 
-#include <cuda.h>
-#include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 
 #include <algorithm>

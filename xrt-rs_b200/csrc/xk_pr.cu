@@ -48,13 +48,13 @@
 #include <vector>
 
 #include "xk_pr.cuh"
+#include "xk_sm100.cuh"
 
 namespace xk {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kSumFields = 26;
-constexpr uint32_t kMaxWaitIters = 1u << 24;
 // Stages of FP32 partial sums per fold into the two-float accumulators.
 constexpr int kFoldStages = 1;
 // |e| bound under which the packed sweep's series reciprocal is used.
@@ -407,52 +407,7 @@ __global__ void finalize_kernel(const double* __restrict__ partial, const int* _
 // Persistent kernel
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
-                                         uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Waits for the barrier phase with an iteration limit; false on time-out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t it = 0; it < kMaxWaitIters; ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void fence_proxy_async() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
+using namespace sm100;  // mbarriers with bounded waits, bulk copies (xk_sm100.cuh)
 
 __device__ __forceinline__ float rcp_approx(float x) {
     float r;

@@ -80,6 +80,7 @@ struct Req {
 
 constexpr int kEpochRing = 3;
 constexpr int kVariants = xk::kPrVariants;
+constexpr int kForkStreams = 4;  // streams the kernel variants of one epoch run on
 constexpr int kPlanBatch = 32;  // requests planned together at most
 
 struct EpochSlot {
@@ -101,6 +102,10 @@ struct xk_server {
     int num_sms = 0;
     cudaStream_t plan_stream = nullptr, exec_stream = nullptr, io_stream = nullptr,
                  f64_stream = nullptr, out_stream = nullptr;
+    // An epoch's launches of different kernel variants touch different
+    // requests, so they run on parallel streams and their tails overlap.
+    cudaStream_t fork_streams[kForkStreams] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kForkStreams] = {};
     std::mutex mu;
     std::condition_variable cv_work, cv_plan, cv_done;
     std::deque<Req*> pending;    // submitted, not admitted
@@ -122,6 +127,7 @@ struct xk_server {
     long long submitted = 0, completed = 0, failed = 0;
     std::atomic<long long> epochs{0}, kernels{0};
     double pairs_done = 0.0;
+    double pairs_launched = 0.0;  // epochs launched (worker thread; read under mu)
     std::string last_error;
 };
 
@@ -373,13 +379,28 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
     unsigned long long* counters = e.ctrl.as<unsigned long long>();
     int* d_err = reinterpret_cast<int*>(e.ctrl.as<char>() + 128);
     const int sms = std::max(1, s->num_sms - std::max(0, s->opts.reserve_sms));
+    XK_CUDA_TRY(cudaEventRecord(s->fork_ev, s->exec_stream));
+    int forks = 0;
     for (int v = 0; v < kVariants; ++v) {
         if (!nsol[v]) continue;
+        cudaStream_t st = s->fork_streams[forks % kForkStreams];
+        if (forks < kForkStreams) XK_CUDA_TRY(cudaStreamWaitEvent(st, s->fork_ev, 0));
         XK_TRY(xk::pr_launch(e.table.as<xk::PrSolve>() + first[v], nsol[v], counts[v], v,
-                             counters + v, d_err, s->exec_stream, sms, 0));
+                             counters + v, d_err, st, sms, 0));
         s->kernels++;
+        ++forks;
+    }
+    for (int f = 0; f < std::min(forks, kForkStreams); ++f) {
+        XK_CUDA_TRY(cudaEventRecord(s->join_ev[f], s->fork_streams[f]));
+        XK_CUDA_TRY(cudaStreamWaitEvent(s->exec_stream, s->join_ev[f], 0));
     }
     XK_CUDA_TRY(cudaMemcpyAsync(e.h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s->exec_stream));
+    double launched = 0.0;
+    for (const Take& t : takes) launched += (double)t.count * t.q->pairs_per_item;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->pairs_launched += launched;
+    }
     for (const Take& t : takes) {
         t.q->next_item += t.count;
         t.q->epochs++;
@@ -593,6 +614,14 @@ void destroy_server(xk_server* s) {
     s->plan_ws.release();
     s->f64ws.rays.release();
     s->f64ws.partials.release();
+    for (int f = 0; f < kForkStreams; ++f) {
+        if (s->fork_streams[f]) {
+            cudaStreamSynchronize(s->fork_streams[f]);
+            cudaStreamDestroy(s->fork_streams[f]);
+        }
+        if (s->join_ev[f]) cudaEventDestroy(s->join_ev[f]);
+    }
+    if (s->fork_ev) cudaEventDestroy(s->fork_ev);
     for (cudaStream_t st : {s->plan_stream, s->exec_stream, s->io_stream, s->f64_stream, s->out_stream})
         if (st) {
             cudaStreamSynchronize(st);
@@ -608,9 +637,9 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
     s->num_sms = ctx->num_sms;
     if (opts) s->opts = *opts;
     if (s->opts.hbm_budget_bytes <= 0) s->opts.hbm_budget_bytes = 120e9;
-    if (s->opts.epoch_pairs <= 0) s->opts.epoch_pairs = 2e10;
+    if (s->opts.epoch_pairs <= 0) s->opts.epoch_pairs = 3e10;
     if (s->opts.max_active <= 0) s->opts.max_active = 64;
-    if (s->opts.item_pairs <= 0) s->opts.item_pairs = 4e6;
+    if (s->opts.item_pairs <= 0) s->opts.item_pairs = 1e6;
     if (s->opts.reserve_sms <= 0) s->opts.reserve_sms = 8;
     s->opts.reserve_sms = std::min(s->opts.reserve_sms, s->num_sms - 1);
     s->pr_opts = ctx->pr_opts;
@@ -624,6 +653,11 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
     XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->io_stream, cudaStreamNonBlocking, hi));
     XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->f64_stream, cudaStreamNonBlocking, lo));
     XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->out_stream, cudaStreamNonBlocking, hi));
+    for (int f = 0; f < kForkStreams; ++f) {
+        XK_CUDA_TRY(cudaStreamCreateWithPriority(&s->fork_streams[f], cudaStreamNonBlocking, lo));
+        XK_CUDA_TRY(cudaEventCreateWithFlags(&s->join_ev[f], cudaEventDisableTiming));
+    }
+    XK_CUDA_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
     for (EpochSlot& e : s->slots) {
         XK_TRY(e.table.ensure(kVariants * (size_t)std::max(1, s->opts.max_active) * sizeof(xk::PrSolve)));
         XK_TRY(e.ctrl.ensure(256));
@@ -815,6 +849,7 @@ int xk_server_get_stats(xk_server* s, xk_server_stats* out) {
     out->pending = (long long)s->pending.size();
     out->active = (long long)s->active.size();
     out->pairs_done = s->pairs_done;
+    out->pairs_launched = s->pairs_launched;
     out->used_bytes = s->used_bytes;
     out->peak_bytes = s->peak_bytes;
     out->resident_ray_bytes = s->ray_bytes;

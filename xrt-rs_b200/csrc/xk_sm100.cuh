@@ -1,10 +1,9 @@
-// sm_100a building blocks in inline PTX: mbarriers with bounded waits, 2-D
-// TMA tile loads, tcgen05 tensor-memory allocation, UMMA issue, commit and
-// tensor-memory loads. Every wait is bounded; a wait that runs out returns
+// sm_100a building blocks in inline PTX: mbarriers with bounded waits, bulk
+// global-to-shared copies, tcgen05 tensor-memory allocation, UMMA issue, commit and tensor-memory
+// loads. Every wait is bounded; a wait that runs out returns
 // false and the caller records an error instead of spinning forever.
 #pragma once
 
-#include <cuda.h>
 #include <stdint.h>
 
 namespace xk {
@@ -31,6 +30,24 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                  : "memory");
 }
 
+// Bulk copy (no multicast) of `bytes` (a multiple of 16, both addresses
+// 16-byte aligned) from global into shared memory, completing `bar`'s
+// transaction count.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy, tensor core) accesses.
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -53,22 +70,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     for (uint32_t it = 0; it < kMaxWaitIters; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
-}
-
-// 2-D tiled TMA load (no multicast) of the box at (x, y) into shared memory,
-// completing `bar`'s transaction count. x is the innermost coordinate in
-// elements; the caller keeps x * element size a multiple of 16 bytes.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
-                                            uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void prefetch_tensor_map(const CUtensorMap* map) {
-    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
 // ---- tensor memory -----------------------------------------------------------

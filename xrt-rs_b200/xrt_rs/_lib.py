@@ -139,7 +139,8 @@ class XkServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong) for n in
                 ("submitted", "completed", "failed", "epochs", "kernels", "pending", "active")] + \
                [(n, ctypes.c_double) for n in
-                ("pairs_done", "used_bytes", "peak_bytes", "resident_ray_bytes")]
+                ("pairs_done", "used_bytes", "peak_bytes", "resident_ray_bytes",
+                 "pairs_launched")]
 
     def to_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
