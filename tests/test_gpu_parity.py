@@ -203,6 +203,31 @@ def test_kirchhoff_gpu_records(ctx, oracle, golden_case):
         assert abs(es2[i] - c) / abs(c) < 1e-4
 
 
+@pytest.mark.parametrize("n_rays,n_pix", [(0, 7), (1, 1), (3001, 257), (40_000, 4099)])
+def test_kirchhoff_gpu_records_match_columns(ctx, n_rays, n_pix):
+    """The record entry point widens on the device and interleaves the field
+    there: identical, bit for bit, to the column entry point on the same
+    (f32-rounded) values; no rays gives a zero field."""
+    rays, pix = synth.config0(seed=3)
+    rng = np.random.default_rng(n_rays + n_pix)
+    ri = rng.integers(0, len(rays["x"]), n_rays)
+    pi = rng.integers(0, len(pix["x"]), n_pix)
+    recs = np.zeros(n_rays, dtype=xrt_rs.GPU_RAY_DTYPE)
+    for k in xrt_rs.GPU_RAY_DTYPE.names:
+        recs[k] = rays[k][ri]
+    px = np.zeros(n_pix, dtype=xrt_rs.GPU_PIXEL_DTYPE)
+    for k in "xyz":
+        px[k] = pix[k][pi]
+    es, ep = xrt_rs.kirchhoff_gpu(ctx, recs, px)
+    wide_r = {k: recs[k].astype(np.float64) for k in cases.RAY_FIELDS}
+    wide_p = {k: px[k].astype(np.float64) for k in "xyz"}
+    out, _ = run(ctx, wide_r, wide_p, "f32pr")
+    assert np.array_equal(es.real, out[0]) and np.array_equal(es.imag, out[1])
+    assert np.array_equal(ep.real, out[2]) and np.array_equal(ep.imag, out[3])
+    if n_rays == 0:
+        assert not np.any(es) and not np.any(ep)
+
+
 @pytest.fixture
 def sweep_ctx(ctx):
     yield ctx

@@ -450,35 +450,47 @@ int xk_kirchhoff_gpu(xk_ctx* ctx, const xk_gpu_ray* rays, size_t n_rays,
     if ((n_rays && !rays) || (n_pix && (!pixels || !out)))
         return fail(ctx, XK_ERR_INVALID, "null pointer");
     if (n_pix == 0) return XK_OK;
-    // Promote the f32 records to f64 SoA (exact), as the reference's host
-    // side promotes them for the base-phase restore (kirchhoff.rs:96-104).
-    std::vector<double> r(12 * n_rays), p(3 * n_pix), o(4 * n_pix);
-    for (size_t i = 0; i < n_rays; ++i) {
-        const xk_gpu_ray& g = rays[i];
-        const float v[12] = {g.x, g.y, g.z, g.nx, g.ny, g.nz, g.nl, g.es_re, g.es_im, g.ep_re,
-                             g.ep_im, g.energy};
-        for (int f = 0; f < 12; ++f) r[f * n_rays + i] = v[f];
-    }
-    for (size_t i = 0; i < n_pix; ++i) {
-        p[i] = pixels[i].x;
-        p[n_pix + i] = pixels[i].y;
-        p[2 * n_pix + i] = pixels[i].z;
-    }
-    const double* b = r.data();
-    xk_rays xr{b, b + n_rays, b + 2 * n_rays, b + 3 * n_rays, b + 4 * n_rays, b + 5 * n_rays,
-               b + 6 * n_rays, b + 7 * n_rays, b + 8 * n_rays, b + 9 * n_rays, b + 10 * n_rays,
-               b + 11 * n_rays};
-    xk_pixels xp{p.data(), p.data() + n_pix, p.data() + 2 * n_pix};
-    xk_field xf{o.data(), o.data() + n_pix, o.data() + 2 * n_pix, o.data() + 3 * n_pix};
-    int rc = xk_diffraction_integral(ctx, &xr, n_rays, &xp, n_pix, &xf, XK_PATH_F32PR, nullptr);
-    if (rc != XK_OK) return rc;
-    for (size_t i = 0; i < n_pix; ++i) {
-        out[4 * i + 0] = o[i];
-        out[4 * i + 1] = o[n_pix + i];
-        out[4 * i + 2] = o[2 * n_pix + i];
-        out[4 * i + 3] = o[3 * n_pix + i];
-    }
-    return XK_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    // The f32 records go to the device as they are (48 + 16 bytes each) and
+    // are widened to f64 SoA there (exact, as the reference's host side
+    // promotes them for the base-phase restore, kirchhoff.rs:96-104); the
+    // field comes back as 4 doubles per pixel.
+    const size_t rec_bytes = n_rays * sizeof(xk_gpu_ray), pix_bytes = n_pix * sizeof(xk_gpu_pixel);
+    const size_t rec_off = 0, pix_off = (rec_bytes + 255) / 256 * 256;
+    const size_t out_off = pix_off + (pix_bytes + 255) / 256 * 256;
+    xk::Status st = ctx->in_beam.ensure(out_off + 4 * n_pix * sizeof(double));
+    if (st.ok()) st = ctx->in_rays.ensure(std::max<size_t>(12 * n_rays * sizeof(double), 8));
+    if (st.ok()) st = ctx->in_pix.ensure(3 * n_pix * sizeof(double));
+    if (st.ok()) st = ctx->out_field.ensure(4 * n_pix * sizeof(double));
+    if (!st.ok()) return fail(ctx, st);
+    char* staging = ctx->in_beam.as<char>();
+    auto* d_rec = reinterpret_cast<xk_gpu_ray*>(staging + rec_off);
+    auto* d_pxr = reinterpret_cast<xk_gpu_pixel*>(staging + pix_off);
+    double* d_out = reinterpret_cast<double*>(staging + out_off);
+    if (n_rays)
+        st = xk::Status::FromCuda(
+            cudaMemcpyAsync(d_rec, rays, rec_bytes, cudaMemcpyHostToDevice, s));
+    if (st.ok())
+        st = xk::Status::FromCuda(
+            cudaMemcpyAsync(d_pxr, pixels, pix_bytes, cudaMemcpyHostToDevice, s));
+    double* cols[12];
+    xk::RaysDev rd;
+    ray_columns(ctx, n_rays, cols, &rd);
+    double* dp = ctx->in_pix.as<double>();
+    if (st.ok()) st = xk::gpu_records_enqueue(d_rec, n_rays, d_pxr, n_pix, cols, dp, dp + n_pix,
+                                              dp + 2 * n_pix, s);
+    xk::PixDev pd{dp, dp + n_pix, dp + 2 * n_pix};
+    double* dout = ctx->out_field.as<double>();
+    xk::FieldDev fd{dout, dout + n_pix, dout + 2 * n_pix, dout + 3 * n_pix};
+    int used = XK_PATH_F32PR;
+    if (st.ok()) st = run_solve(ctx, rd, n_rays, pd, n_pix, fd, XK_PATH_F32PR, s, nullptr, &used);
+    if (st.ok()) st = xk::interleave_field_enqueue(fd, n_pix, d_out, s);
+    if (st.ok()) st = xk::Status::FromCuda(cudaMemcpyAsync(out, d_out, 4 * n_pix * sizeof(double),
+                                                           cudaMemcpyDeviceToHost, s));
+    if (st.ok()) st = xk::Status::FromCuda(cudaStreamSynchronize(s));
+    return st.ok() ? XK_OK : fail(ctx, st);
 }
 
 int xk_kirchhoff_auto(const xk_gpu_ray* rays, size_t n_rays, const xk_gpu_pixel* pixels,

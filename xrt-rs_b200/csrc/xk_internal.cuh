@@ -194,4 +194,13 @@ FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms);
 Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t stream,
                        int num_sms, int path, FresnelReport* rep);
 
+// GpuRay / GpuPixel records (f32 AoS, src/gpu/kirchhoff.rs:20-45) on the
+// device -> the f64 SoA columns the solvers read (exact widening), and the
+// solved field -> 4 doubles per pixel, the layout of Vec<(Complex64,
+// Complex64)> (xk_wave.cu).
+Status gpu_records_enqueue(const xk_gpu_ray* rays, size_t n, const xk_gpu_pixel* pix, size_t m,
+                           double* const ray_cols[12], double* px, double* py, double* pz,
+                           cudaStream_t stream);
+Status interleave_field_enqueue(const FieldDev& f, size_t m, double* out, cudaStream_t stream);
+
 }  // namespace xk

@@ -101,4 +101,56 @@ Status beam_rays_enqueue(const BeamDev& beam, const uint64_t* good, size_t n_goo
     return Status::Ok();
 }
 
+namespace {
+
+__global__ void __launch_bounds__(kThreads)
+    gpu_records_kernel(const xk_gpu_ray* __restrict__ rays, size_t n,
+                       const xk_gpu_pixel* __restrict__ pix, size_t m, RayCols cols, double* px,
+                       double* py, double* pz) {
+    const size_t stride = (size_t)gridDim.x * kThreads;
+    for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < n; i += stride) {
+        const xk_gpu_ray r = rays[i];
+        // GpuRay order x, y, z, nx, ny, nz, nl, energy, es, ep -> RaysDev order.
+        const float v[12] = {r.x, r.y, r.z, r.nx, r.ny, r.nz, r.nl,
+                             r.es_re, r.es_im, r.ep_re, r.ep_im, r.energy};
+#pragma unroll
+        for (int f = 0; f < 12; ++f) cols.c[f][i] = (double)v[f];
+    }
+    for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < m; i += stride) {
+        const xk_gpu_pixel p = pix[i];
+        px[i] = (double)p.x;
+        py[i] = (double)p.y;
+        pz[i] = (double)p.z;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) interleave_kernel(FieldDev f, size_t m,
+                                                              double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < m;
+         i += (size_t)gridDim.x * kThreads)
+        reinterpret_cast<double4*>(out)[i] = make_double4(f.es_re[i], f.es_im[i], f.ep_re[i],
+                                                          f.ep_im[i]);
+}
+
+}  // namespace
+
+Status gpu_records_enqueue(const xk_gpu_ray* rays, size_t n, const xk_gpu_pixel* pix, size_t m,
+                           double* const ray_cols[12], double* px, double* py, double* pz,
+                           cudaStream_t stream) {
+    if (n == 0 && m == 0) return Status::Ok();
+    RayCols cols;
+    for (int f = 0; f < 12; ++f) cols.c[f] = ray_cols[f];
+    gpu_records_kernel<<<grid_for(std::max(n, m)), kThreads, 0, stream>>>(rays, n, pix, m, cols,
+                                                                          px, py, pz);
+    XK_CUDA_TRY(cudaGetLastError());
+    return Status::Ok();
+}
+
+Status interleave_field_enqueue(const FieldDev& f, size_t m, double* out, cudaStream_t stream) {
+    if (m == 0) return Status::Ok();
+    interleave_kernel<<<grid_for(m), kThreads, 0, stream>>>(f, m, out);
+    XK_CUDA_TRY(cudaGetLastError());
+    return Status::Ok();
+}
+
 }  // namespace xk
