@@ -39,6 +39,10 @@ def test_version_and_status_strings():
     assert b"sm_100a" in lib.xk_version()
     for code in range(10):
         assert lib.xk_status_string(code)
+    assert xrt_rs.route_reason(0) == ""
+    assert xrt_rs.route_reason(1) == "no rays"
+    assert xrt_rs.route_reason(7) == "non-finite ray or screen values"
+    assert xrt_rs.route_reason(8) == "unknown"
 
 
 def test_length_mismatch_raises_value_error():

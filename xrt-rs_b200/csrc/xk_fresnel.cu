@@ -498,7 +498,10 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
                          std::max(0.5 * std::fabs(in.x_max - in.x_min) * in.max_rx_off,
                                   0.5 * std::fabs(in.z_max - in.z_min) * in.max_rz_off);
     rep->used_path = path;
-    if (path == XK_PATH_SEPARABLE && n && in.max_amp != 0.0 && !(cross < 2097152.0))
+    // Non-finite inputs take the FP64 sum, which propagates them as
+    // fresnel.rs:53-106 does.
+    if (path == XK_PATH_SEPARABLE && n &&
+        (!in.finite || (in.max_amp != 0.0 && !(cross < 2097152.0))))
         rep->used_path = path = XK_PATH_F64;
     if (path == XK_PATH_F64 || n == 0 || in.max_amp == 0.0) {
         // FP64 direct sum (with no rays or zero amplitudes it writes zeros).
@@ -591,17 +594,19 @@ xk::Status fresnel_host(xk_ctx* ctx, const double* rx, const double* rz, const d
         XK_CUDA_TRY(cudaMemcpyAsync(d + f * n, src[f], nb, cudaMemcpyHostToDevice, s));
     double max_amp = 0.0, max_rx = 0.0, max_rz = 0.0;
     const double ox = 0.5 * (sc->x_min + sc->x_max), oz = 0.5 * (sc->z_min + sc->z_max);
+    bool finite = true;
     for (size_t j = 0; j < n; ++j) {
         // An upper bound of |es_j| is all the f16 scaling needs.
         max_amp = std::max(max_amp, std::max(std::fabs(er[j]), std::fabs(ei[j])));
         max_rx = std::max(max_rx, std::fabs(rx[j] - ox));
         max_rz = std::max(max_rz, std::fabs(rz[j] - oz));
+        finite = finite && std::isfinite(rx[j] + rz[j] + er[j] + ei[j]);
     }
     max_amp *= 1.4142135623730951;
     double* out = ctx->out_field.as<double>();
     xk::FresnelIn in{d, d + n, d + 2 * n, d + 3 * n, n, energy, dist,
                      sc->x_min, sc->x_max, sc->z_min, sc->z_max, nx, nz, max_amp, max_rx, max_rz,
-                     out, out + m};
+                     out, out + m, finite};
     xk::FresnelReport rep;
     cudaEvent_t g0 = nullptr, g1 = nullptr;
     if (stats && path == XK_PATH_SEPARABLE) {

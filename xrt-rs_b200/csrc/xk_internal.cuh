@@ -165,6 +165,7 @@ struct FresnelIn {
     double max_amp;                   // max_j |es_j| (scales the f16 factors)
     double max_rx_off, max_rz_off;    // max_j |x_j - screen centre x|, same for z
     double *out_re, *out_im;          // device, nx * nz each
+    bool finite = true;               // every ray coordinate and amplitude is finite
 };
 
 struct FresnelShape {

@@ -54,7 +54,7 @@ namespace xk {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kSumFields = 26;
+constexpr int kSumFields = 27;
 // Stages of FP32 partial sums per fold into the two-float accumulators.
 constexpr int kFoldStages = 1;
 // |e| bound under which the packed sweep's series reciprocal is used.
@@ -73,15 +73,18 @@ __constant__ int c_sum_ops[kSumFields] = {
     OP_MIN, OP_MAX,                                  // energy range
     OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX,  // normal range
     OP_SUM, OP_SUM, OP_SUM,                          // screen position sums
-    OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX}; // screen bbox
-const int h_sum_ops[kSumFields] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 1, 2, 1, 1,
-                                   1, 2, 2, 2, 0, 0, 0, 1, 1, 1, 2, 2, 2};
+    OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX,  // screen bbox
+    OP_SUM};                                         // non-finite probe
+const int h_sum_ops[kSumFields] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 1, 2, 1, 1, 1,
+                                   2, 2, 2, 0, 0, 0, 1, 1, 1, 2, 2, 2, 0};
 
 __device__ __forceinline__ double op_combine(int op, double a, double b) {
     return op == OP_SUM ? a + b : (op == OP_MIN ? fmin(a, b) : fmax(a, b));
 }
 
-// One partial summary per block over rays and screen points.
+// One partial summary per block over rays and screen points. The last field
+// sums every input value times zero: 0 when all are finite, NaN otherwise
+// (fmin / fmax skip NaN, so the boxes alone would not show it).
 __global__ void __launch_bounds__(256) summary_kernel(RaysDev r, int n, PixDev p, int m,
                                                      double* __restrict__ block_out) {
     double f[kSumFields];
@@ -97,12 +100,15 @@ __global__ void __launch_bounds__(256) summary_kernel(RaysDev r, int n, PixDev p
         f[9] = fmin(f[9], e); f[10] = fmax(f[10], e);
         f[11] = fmin(f[11], a); f[12] = fmin(f[12], b); f[13] = fmin(f[13], c);
         f[14] = fmax(f[14], a); f[15] = fmax(f[15], b); f[16] = fmax(f[16], c);
+        f[26] += (x + y + z + e + a + b + c + r.nl[i] + r.es_re[i] + r.es_im[i] + r.ep_re[i] +
+                  r.ep_im[i]) * 0.0;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
         double x = p.x[i], y = p.y[i], z = p.z[i];
         f[17] += x; f[18] += y; f[19] += z;
         f[20] = fmin(f[20], x); f[21] = fmin(f[21], y); f[22] = fmin(f[22], z);
         f[23] = fmax(f[23], x); f[24] = fmax(f[24], y); f[25] = fmax(f[25], z);
+        f[26] += (x + y + z) * 0.0;
     }
     __shared__ double sm[8][kSumFields];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1106,7 +1112,8 @@ const char* const kRouteReasons[kRouteReasonCount] = {
     "non-positive energy",
     "ray and screen bounding boxes overlap",
     "no cell size meets the phase budget",
-    "ray cell grid too fine"};
+    "ray cell grid too fine",
+    "non-finite ray or screen values"};
 
 Status PrWorkspace::ensure_host(size_t bytes) {
     if (bytes <= host_bytes) return Status::Ok();
@@ -1241,6 +1248,13 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             I.f[i] = v;
         }
         const double* f = I.f;
+        if (!(f[26] == 0.0)) {
+            // NaN or infinite inputs: the FP64 sum propagates them the way
+            // diffraction.rs:67-117 does; the planner's geometry would not.
+            P.routed = true;
+            P.route_reason = 7;
+            continue;
+        }
         if (!(f[9] == f[10])) {
             P.routed = true;
             P.route_reason = 2;

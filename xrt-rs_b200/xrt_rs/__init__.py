@@ -28,7 +28,7 @@ __all__ = [
     "GpuContext", "kirchhoff_gpu", "kirchhoff_auto", "GPU_RAY_DTYPE", "GPU_PIXEL_DTYPE",
     "XkError", "XK_PATH_F64", "XK_PATH_F32PR", "RAY_FIELDS", "PIXEL_FIELDS", "Batch",
     "autotune", "WaveParams", "prepare_wave", "beam_to_diffraction_rays", "diffraction_from_beam",
-    "FresnelScreen", "FresnelResult", "fresnel_propagate",
+    "FresnelScreen", "FresnelResult", "fresnel_propagate", "route_reason",
 ]
 
 RAY_FIELDS = ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re", "ep_im", "energy")
@@ -43,6 +43,11 @@ GPU_PIXEL_DTYPE = np.dtype([(n, np.float32) for n in ("x", "y", "z", "_pad")])
 
 _PATHS = {"f64": XK_PATH_F64, "f32pr": XK_PATH_F32PR, XK_PATH_F64: XK_PATH_F64,
           XK_PATH_F32PR: XK_PATH_F32PR}
+
+
+def route_reason(code: int) -> str:
+    """Why an f32pr request ran on the FP64 path (stats ``routed_reason``)."""
+    return _lib.load().xk_route_reason(int(code)).decode()
 
 
 def _path(path) -> int:
