@@ -44,6 +44,10 @@ UNIT = "Gpair/s"
 # operations and 4 SFU operations (rsqrt, rcp, sin, cos).
 FMA_OPS_PER_PAIR = 34
 SFU_OPS_PER_PAIR = 4
+# DRAM bytes (read + write) of one pr_persistent_kernel launch on the 2^20 x
+# 512^2 workload from an ncu capture of the full-size launch, by the number of
+# amplitude columns summed (two-column kernel: key False).
+DRAM_BYTES_CONFIG1 = {False: 513.6e6, True: None}
 FMA_LANES_PER_SM = 128
 SFU_LANES_PER_SM = 16
 
@@ -62,6 +66,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sweep", type=int, default=-1, help="-1 auto, 0 SFU reciprocal, 1 packed")
     ap.add_argument("--phase-budget", type=float, default=512.0)
+    ap.add_argument("--polarization", type=int, default=-1, choices=[-1, 0],
+                    help="-1: one amplitude column when all rays share a polarization; "
+                         "0: always sum Es and Ep separately")
     ap.add_argument("--workload", choices=["single", "batch", "sweep", "serve", "fresnel"],
                     default="single",
                     help="single: the 2^20 x 512^2 solve (default); batch: 64 uneven solves; "
@@ -225,6 +232,7 @@ def run_batch(args):
     ctx = xrt_rs.GpuContext.new(0)
     ctx.set_option("sweep", args.sweep)
     ctx.set_option("phase_budget", args.phase_budget)
+    ctx.set_option("polarization", args.polarization)
     solves = synth.config3(seed=0, count=args.batch_count)
     pairs = float(sum(len(r["x"]) * len(p["x"]) for r, p, _ in solves))
     dev = []
@@ -305,6 +313,7 @@ def run_sweep(args):
     ctx = xrt_rs.GpuContext.new(0)
     ctx.set_option("sweep", args.sweep)
     ctx.set_option("phase_budget", args.phase_budget)
+    ctx.set_option("polarization", args.polarization)
     cells = []
     for e in synth.CONFIG2_ENERGIES:
         for d in synth.CONFIG2_DISTANCES:
@@ -344,6 +353,7 @@ def run_sweep(args):
                 "energy_ev": e, "dist_mm": d, "sigma_mm": meta["sigma_mm"],
                 "radius_mm": meta["radius_mm"], "path": "f32pr" if f32[2]["path"] == 1 else "f64",
                 "n_chunks": f32[2]["n_chunks"], "sweep": f32[2]["sweep"],
+                "amplitude_columns": 1 if f32[2]["one_polarization"] else 2,
                 "rel_l2_field": e32, "rel_l2_intensity": e32i,
                 "fp64_formula_rel_l2_field": e64, "fp64_formula_rel_l2_intensity": e64i,
                 "f32pr_gpair_s": pairs / f32[1] / 1e6, "fp64_gpair_s": pairs / f64[1] / 1e6,
@@ -603,6 +613,7 @@ def main():
         raise RuntimeError("no CUDA device")
     ctx.set_option("sweep", args.sweep)
     ctx.set_option("phase_budget", args.phase_budget)
+    ctx.set_option("polarization", args.polarization)
 
     rays, screen = synth.config1(seed=rank, n_rays=args.rays, grid=args.grid)
     fields = xrt_rs.RAY_FIELDS
@@ -718,21 +729,34 @@ def main():
     props = torch.cuda.get_device_properties(dev)
     sms = props.multi_processor_count
     clk_mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
-    pair_per_clk_sm = min(FMA_LANES_PER_SM / FMA_OPS_PER_PAIR, SFU_LANES_PER_SM / SFU_OPS_PER_PAIR)
+    # With one common polarization the algorithm has one complex multiply-add
+    # per pair instead of two (4 FMA-pipe ops fewer).
+    one_col = bool(stats["one_polarization"])
+    fma_ops = FMA_OPS_PER_PAIR - (4 if one_col else 0)
+    pair_per_clk_sm = min(FMA_LANES_PER_SM / fma_ops, SFU_LANES_PER_SM / SFU_OPS_PER_PAIR)
     peak = sms * pair_per_clk_sm * clk_mhz * 1e6 / 1e9
     kms = float(np.mean(kern_ms))
     achieved = pairs / (kms / 1e3) / 1e9
     # DRAM bytes (read + write) of one pr_persistent_kernel launch on this
     # workload, from an ncu capture of the full-size launch
     # (profiles/pr_persistent_config1_dram.md); other sizes report null.
-    traffic = 513.6e6 if (n == 1 << 20 and args.grid == 512 and args.phase_budget == 512.0) else None
+    full_size = n == 1 << 20 and args.grid == 512 and args.phase_budget == 512.0
+    traffic = (DRAM_BYTES_CONFIG1[one_col] if full_size else None)
     roofline = {"bound": "fp32_sfu", "achieved": achieved, "peak": peak, "unit": UNIT,
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel": "pr_persistent_kernel", "kernel_ms": kms,
-                "peak_source": (f"{sms} SMs x min(128 FP32 lanes / {FMA_OPS_PER_PAIR} FMA-pipe ops, "
+                "peak_source": (f"{sms} SMs x min(128 FP32 lanes / {fma_ops} FMA-pipe ops, "
                                 f"16 SFU lanes / {SFU_OPS_PER_PAIR} SFU ops) per pair x "
                                 f"{clk_mhz:.0f} MHz median SM clock sampled in the timed region"),
-                "algorithmic_ops_per_pair": {"fma_pipe": FMA_OPS_PER_PAIR, "sfu": SFU_OPS_PER_PAIR}}
+                "algorithmic_ops_per_pair": {"fma_pipe": fma_ops, "sfu": SFU_OPS_PER_PAIR}}
+    if stats["sweep"] == 1:
+        # The packed uniform-normal sweep as issued: FMA-pipe cycles per pair
+        # (an f32x2 instruction holds the pipe two cycles for two pairs) and
+        # MUFU operations per pair.
+        cyc = 17 if one_col else 21
+        ceil = sms * min(FMA_LANES_PER_SM / cyc, SFU_LANES_PER_SM / 2) * clk_mhz * 1e6 / 1e9
+        roofline["kernel_issue_ceiling"] = {"fma_pipe_cycles_per_pair": cyc, "mufu_per_pair": 2,
+                                            "value": ceil, "frac": achieved / ceil}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -748,7 +772,8 @@ def main():
                    "parallelism": f"replica x{world}", "l2": "flushed between steps (256 MiB write)",
                    "path": "f32pr", "phase_bound_rad": stats["phase_bound_rad"],
                    "n_tiles": stats["n_tiles"], "n_chunks": stats["n_chunks"],
-                   "groups": stats["groups"], "sweep": ["sfu_rcp", "packed_f32x2"][stats["sweep"]]},
+                   "groups": stats["groups"], "sweep": ["sfu_rcp", "packed_f32x2"][stats["sweep"]],
+                   "amplitude_columns": 1 if stats["one_polarization"] else 2},
         "e2e": e2e, "fp64_plain": fp64, "roofline": roofline, "cpu_baseline": cpu,
         "clocks": clk, "gpu_launches": launches,
     }

@@ -108,6 +108,8 @@ typedef struct xk_stats {
     int groups;              /* ray groups per tile (F32PR) */
     int routed_reason;       /* 0 = not routed; see xk_route_reason() */
     int sweep;               /* F32PR sweep used: 0 SFU reciprocal, 1 packed + series, -1 none */
+    int one_polarization;    /* F32PR: 1 if every ray had ray 0's polarization, so the kernel
+                                summed one amplitude column and Ep = (ep_0 / es_0) Es */
 } xk_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -145,6 +147,9 @@ const char* xk_route_reason(int reason);
  *   "sweep"          -1 automatic, 0 SFU reciprocal, 1 packed f32x2 sweep
  *   "groups"         ray ranges per screen tile, 0 = automatic
  *   "items_per_warp" target work items per resident warp (automatic groups)
+ *   "polarization"   -1 (default): when every ray's (es, ep) is a multiple of
+ *                    ray 0's (to 2^-24), sum one amplitude column and scale it
+ *                    for Es and Ep; 0: always sum Es and Ep separately
  *   "f64_reduction"  XK_PATH_F64 only: 0 (default) evaluates sin/cos of each
  *                    FP64 phase with the library functions, as the reference
  *                    does; 1 first reduces the phase by 2 pi with an FMA-based
@@ -325,6 +330,7 @@ typedef struct xk_batch_stats {
 typedef struct xk_solve_plan {
     int path, routed_reason, n_tiles, n_chunks, groups, sweep;
     double phase_bound_rad;
+    int one_polarization;
 } xk_solve_plan;
 
 /* Copies host inputs to the device (unless XK_BATCH_DEVICE), plans every

@@ -123,6 +123,7 @@ xk::Status run_solve(xk_ctx* ctx, const xk::RaysDev& rays, size_t n_rays, const 
             stats->routed_reason = P.routed ? P.route_reason : 0;
             stats->main_kernel_ms = er.main_kernel_ms;
             stats->sweep = P.routed ? -1 : (P.fast ? 1 : 0);
+            stats->one_polarization = !P.routed && P.one_pol;
         }
     } else {
         XK_TRY(xk::f64_enqueue(rays, n_rays, pix, n_pix, out, ctx->f64ws, stream, ctx->num_sms,
@@ -323,6 +324,10 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
     } else if (n == "f64_reduction") {
         if (value != 0.0 && value != 1.0) return fail(ctx, XK_ERR_INVALID, "f64_reduction is 0 or 1");
         ctx->f64ws.fast_reduction = value != 0.0;
+    } else if (n == "polarization") {
+        if (value != -1.0 && value != 0.0)
+            return fail(ctx, XK_ERR_INVALID, "polarization must be -1 or 0");
+        ctx->pr_opts.polarization = (int)value;
     } else if (n == "items_per_warp") {
         if (value < 1.0 || value > 4096.0) return fail(ctx, XK_ERR_INVALID, "items_per_warp out of range");
         ctx->pr_opts.items_per_warp = (long long)value;

@@ -54,13 +54,18 @@ namespace xk {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kSumFields = 27;
+constexpr int kSumFields = 32;
 // Stages of FP32 partial sums per fold into the two-float accumulators.
 constexpr int kFoldStages = 1;
 // |e| bound under which the packed sweep's series reciprocal is used.
 constexpr double kSeriesRcpBound = 2e-3;
 // Fold the base phase when the estimated chunks per ray group reach this.
 constexpr double kFoldChunksPerGroup = 4.0;
+// Largest |es_j ep_0 - ep_j es_0| / (|es_j| |ep_0| + |ep_j| |es_0|) over the
+// rays under which every ray counts as having ray 0's polarization (2^-24:
+// the per-ray deviation is then below the FP32 rounding of the amplitudes
+// that the kernel applies anyway).
+constexpr double kOnePolTol = 5.9604644775390625e-8;
 
 // ---------------------------------------------------------------------------
 // Planner kernels
@@ -74,9 +79,11 @@ __constant__ int c_sum_ops[kSumFields] = {
     OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX,  // normal range
     OP_SUM, OP_SUM, OP_SUM,                          // screen position sums
     OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX,  // screen bbox
-    OP_SUM};                                         // non-finite probe
-const int h_sum_ops[kSumFields] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 1, 2, 1, 1, 1,
-                                   2, 2, 2, 0, 0, 0, 1, 1, 1, 2, 2, 2, 0};
+    OP_SUM,                                          // non-finite probe
+    OP_MAX,                                          // polarization deviation
+    OP_SUM, OP_SUM, OP_SUM, OP_SUM};                 // ray 0's es, ep
+const int h_sum_ops[kSumFields] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 1, 2, 1, 1, 1, 2, 2,
+                                   2, 0, 0, 0, 1, 1, 1, 2, 2, 2, 0, 2, 0, 0, 0, 0};
 
 __device__ __forceinline__ double op_combine(int op, double a, double b) {
     return op == OP_SUM ? a + b : (op == OP_MIN ? fmin(a, b) : fmax(a, b));
@@ -84,13 +91,17 @@ __device__ __forceinline__ double op_combine(int op, double a, double b) {
 
 // One partial summary per block over rays and screen points. The last field
 // sums every input value times zero: 0 when all are finite, NaN otherwise
-// (fmin / fmax skip NaN, so the boxes alone would not show it).
+// (fmin / fmax skip NaN, so the boxes alone would not show it). Fields 27-31
+// test whether all rays share ray 0's polarization: the largest relative
+// |es_j ep_0 - ep_j es_0|, and ray 0's (es, ep).
 __global__ void __launch_bounds__(256) summary_kernel(RaysDev r, int n, PixDev p, int m,
                                                      double* __restrict__ block_out) {
     double f[kSumFields];
     for (int i = 0; i < kSumFields; ++i)
         f[i] = c_sum_ops[i] == OP_SUM ? 0.0 : (c_sum_ops[i] == OP_MIN ? INFINITY : -INFINITY);
     const int stride = gridDim.x * blockDim.x;
+    const double a0r = r.es_re[0], a0i = r.es_im[0], b0r = r.ep_re[0], b0i = r.ep_im[0];
+    const double a0n = sqrt(a0r * a0r + a0i * a0i), b0n = sqrt(b0r * b0r + b0i * b0i);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         double x = r.x[i], y = r.y[i], z = r.z[i], e = r.energy[i];
         double a = r.nx[i], b = r.ny[i], c = r.nz[i];
@@ -100,8 +111,19 @@ __global__ void __launch_bounds__(256) summary_kernel(RaysDev r, int n, PixDev p
         f[9] = fmin(f[9], e); f[10] = fmax(f[10], e);
         f[11] = fmin(f[11], a); f[12] = fmin(f[12], b); f[13] = fmin(f[13], c);
         f[14] = fmax(f[14], a); f[15] = fmax(f[15], b); f[16] = fmax(f[16], c);
-        f[26] += (x + y + z + e + a + b + c + r.nl[i] + r.es_re[i] + r.es_im[i] + r.ep_re[i] +
-                  r.ep_im[i]) * 0.0;
+        const double ar = r.es_re[i], ai = r.es_im[i], br = r.ep_re[i], bi = r.ep_im[i];
+        f[26] += (x + y + z + e + a + b + c + r.nl[i] + ar + ai + br + bi) * 0.0;
+        const double dr = (ar * b0r - ai * b0i) - (br * a0r - bi * a0i);
+        const double di = (ar * b0i + ai * b0r) - (br * a0i + bi * a0r);
+        const double nrm = sqrt(ar * ar + ai * ai) * b0n + sqrt(br * br + bi * bi) * a0n;
+        const double dn = sqrt(dr * dr + di * di);
+        f[27] = fmax(f[27], nrm > 0.0 ? dn / nrm : (dn > 0.0 ? INFINITY : 0.0));
+        if (i == 0) {
+            f[28] += ar;
+            f[29] += ai;
+            f[30] += br;
+            f[31] += bi;
+        }
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
         double x = p.x[i], y = p.y[i], z = p.z[i];
@@ -391,12 +413,28 @@ __global__ void __launch_bounds__(1024) group_order_kernel(const int* __restrict
 
 // Adds the groups' slots of every tile slot in order and scatters the sum to
 // the screen point's original index.
+// One-polarization solves hold A in components 0 and 1; the field is
+// (pes * A, pep * A).
 __global__ void finalize_kernel(const double* __restrict__ partial, const int* __restrict__ tile_perm,
-                                int groups, int slots, FieldDev out) {
+                                int groups, int slots, FieldDev out, int one_pol, double2 pes,
+                                double2 pep) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= slots) return;
     int id = tile_perm[s];
     if (id < 0) return;
+    if (one_pol) {
+        double ar = 0.0, ai = 0.0;
+        for (int g = 0; g < groups; ++g) {
+            const double* b = partial + (size_t)g * 4 * slots;
+            ar += b[s];
+            ai += b[(size_t)slots + s];
+        }
+        out.es_re[id] = pes.x * ar - pes.y * ai;
+        out.es_im[id] = pes.x * ai + pes.y * ar;
+        out.ep_re[id] = pep.x * ar - pep.y * ai;
+        out.ep_im[id] = pep.x * ai + pep.y * ar;
+        return;
+    }
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int g = 0; g < groups; ++g) {
         const double* b = partial + (size_t)g * 4 * slots;
@@ -555,6 +593,7 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
 // Unfolded variants, at every chunk boundary and at the item end: multiplies
 // the lane's two-float chunk sums by the chunk phasor in FP64, adds them to
 // the item's slots (tile-slot order) and clears the sums.
+template <bool POL>
 __device__ __forceinline__ void flush_chunk(const PrSolve& sv, int t, int g, int lane,
                                             WarpShared& ws) {
     const size_t slots = (size_t)sv.n_tiles * kPrTile;
@@ -566,7 +605,7 @@ __device__ __forceinline__ void flush_chunk(const PrSolve& sv, int t, int g, int
         const double phr = ph.x, phi = ph.y;
         double v[4];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < (POL ? 2 : 4); ++c) {
             v[c] = (double)ws.hi[i * 4 + c][lane] + (double)ws.lo[i * 4 + c][lane];
             ws.hi[i * 4 + c][lane] = 0.f;
             ws.lo[i * 4 + c][lane] = 0.f;
@@ -575,13 +614,16 @@ __device__ __forceinline__ void flush_chunk(const PrSolve& sv, int t, int g, int
         // form only lets the warp go on without waiting for the loads.
         atomicAdd(base + 0 * slots + s, v[0] * phr - v[1] * phi);
         atomicAdd(base + 1 * slots + s, v[0] * phi + v[1] * phr);
-        atomicAdd(base + 2 * slots + s, v[2] * phr - v[3] * phi);
-        atomicAdd(base + 3 * slots + s, v[2] * phi + v[3] * phr);
+        if (!POL) {
+            atomicAdd(base + 2 * slots + s, v[2] * phr - v[3] * phi);
+            atomicAdd(base + 3 * slots + s, v[2] * phi + v[3] * phr);
+        }
     }
 }
 
 // Folded variants, once at the item end: multiplies the lane's two-float
 // sums of the item by i k / (2 pi) in FP64 and adds them to the item's slots.
+template <bool POL>
 __device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int lane,
                                              WarpShared& ws) {
     const size_t slots = (size_t)sv.n_tiles * kPrTile;
@@ -592,20 +634,24 @@ __device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int 
         const size_t s = (size_t)t * kPrTile + lane + 32 * i;
         double v[4];
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+        for (int c = 0; c < (POL ? 2 : 4); ++c)
             v[c] = (double)ws.hi[i * 4 + c][lane] + (double)ws.lo[i * 4 + c][lane];
         // Sub-items of one (group, tile) add into the same slots in sub
         // order (never two in one launch); the atomic form only lets the warp
         // go on without waiting for the loads.
         atomicAdd(base + 0 * slots + s, -kt * v[1]);
         atomicAdd(base + 1 * slots + s, kt * v[0]);
-        atomicAdd(base + 2 * slots + s, -kt * v[3]);
-        atomicAdd(base + 3 * slots + s, kt * v[2]);
+        if (!POL) {
+            atomicAdd(base + 2 * slots + s, -kt * v[3]);
+            atomicAdd(base + 3 * slots + s, kt * v[2]);
+        }
     }
 }
 
 // Prepares the stage's rays for the item direction (lane j handles rays
 // j, j+32).
+// One-polarization kernels (POL) prepare the one amplitude column they sum.
+template <bool POL>
 __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, const PrSolve& sv,
                                            const WarpShared& ws) {
     const double ux = ws.ux, uy = ws.uy, uz = ws.uz;
@@ -622,8 +668,14 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
         float w = (float)(-2.0 * ur);
         float4 a = make_float4(rxf, ryf, rzf, (float)(sv.k * perp2));
         float4 b = make_float4(w, -2.f * (r.nx * rxf + r.ny * ryf + r.nz * rzf), r.nl, -w);
-        float4 e = make_float4(r.es_re * cs - r.es_im * sn, r.es_re * sn + r.es_im * cs,
-                               r.ep_re * cs - r.ep_im * sn, r.ep_re * sn + r.ep_im * cs);
+        float4 e;
+        if (POL) {
+            const float pr = sv.amp_src ? r.ep_re : r.es_re, pi = sv.amp_src ? r.ep_im : r.es_im;
+            e = make_float4(pr * cs - pi * sn, pr * sn + pi * cs, 0.f, 0.f);
+        } else {
+            e = make_float4(r.es_re * cs - r.es_im * sn, r.es_re * sn + r.es_im * cs,
+                            r.ep_re * cs - r.ep_im * sn, r.ep_re * sn + r.ep_im * cs);
+        }
         float4 nn = make_float4(2.f * r.nx, 2.f * r.ny, 2.f * r.nz, 0.f);
         float4* o = reinterpret_cast<float4*>(buf + j);
         o[0] = a;
@@ -635,12 +687,13 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
 
 // Adds the lane's FP32 partials into its two-float accumulators and clears
 // them (every kFoldStages stages and at chunk and item ends).
-template <bool UNIFORM>
+// One-polarization kernels (POL) carry components 0 and 1 only.
+template <bool POL, bool UNIFORM>
 __device__ __forceinline__ void fold_acc(ScalarState<UNIFORM>& ls, WarpShared& ws, int lane) {
 #pragma unroll
     for (int i = 0; i < kPrPpl; ++i)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < (POL ? 2 : 4); ++c) {
             float hi = ws.hi[i * 4 + c][lane], lo = ws.lo[i * 4 + c][lane];
             two_sum_acc(hi, lo, ls.acc[i][c]);
             ws.hi[i * 4 + c][lane] = hi;
@@ -649,12 +702,12 @@ __device__ __forceinline__ void fold_acc(ScalarState<UNIFORM>& ls, WarpShared& w
         }
 }
 
-template <bool UNIFORM>
+template <bool POL, bool UNIFORM>
 __device__ __forceinline__ void fold_acc(PackedState<UNIFORM>& ls, WarpShared& ws, int lane) {
 #pragma unroll
     for (int i = 0; i < kPrPpl / 2; ++i)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < (POL ? 2 : 4); ++c) {
             const float2 v = ls.acc[i][c];
             float hi0 = ws.hi[(2 * i) * 4 + c][lane], lo0 = ws.lo[(2 * i) * 4 + c][lane];
             float hi1 = ws.hi[(2 * i + 1) * 4 + c][lane], lo1 = ws.lo[(2 * i + 1) * 4 + c][lane];
@@ -685,7 +738,7 @@ __device__ __forceinline__ void clear_acc(PackedState<UNIFORM>& ls) {
 }
 
 // SFU sweep: one point per FP32 instruction, rcp.approx for the reciprocal.
-template <bool UNIFORM, bool FOLD>
+template <bool UNIFORM, bool FOLD, bool POL>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
                                             ScalarState<UNIFORM>& ls, WarpShared& ws) {
     const float4* rec = reinterpret_cast<const float4*>(buf);
@@ -716,14 +769,16 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             const float ac = amp * cs, as = amp * sn;
             ls.acc[i][0] = fmaf(e.x, ac, fmaf(-e.y, as, ls.acc[i][0]));
             ls.acc[i][1] = fmaf(e.x, as, fmaf(e.y, ac, ls.acc[i][1]));
-            ls.acc[i][2] = fmaf(e.z, ac, fmaf(-e.w, as, ls.acc[i][2]));
-            ls.acc[i][3] = fmaf(e.z, as, fmaf(e.w, ac, ls.acc[i][3]));
+            if (!POL) {
+                ls.acc[i][2] = fmaf(e.z, ac, fmaf(-e.w, as, ls.acc[i][2]));
+                ls.acc[i][3] = fmaf(e.z, as, fmaf(e.w, ac, ls.acc[i][3]));
+            }
         }
     }
 }
 
 // Packed sweep: two points per f32x2 instruction, series reciprocal.
-template <bool UNIFORM, bool FOLD>
+template <bool UNIFORM, bool FOLD, bool POL>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
                                             PackedState<UNIFORM>& ls, WarpShared& ws) {
     constexpr int H = kPrPpl / 2;
@@ -764,8 +819,10 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             const float2 as = __fmul2_rn(amp, f2(s0, s1));
             ls.acc[i][0] = __ffma2_rn(ex, ac, __ffma2_rn(ney, as, ls.acc[i][0]));
             ls.acc[i][1] = __ffma2_rn(ex, as, __ffma2_rn(ey, ac, ls.acc[i][1]));
-            ls.acc[i][2] = __ffma2_rn(ez, ac, __ffma2_rn(new_, as, ls.acc[i][2]));
-            ls.acc[i][3] = __ffma2_rn(ez, as, __ffma2_rn(ew, ac, ls.acc[i][3]));
+            if (!POL) {
+                ls.acc[i][2] = __ffma2_rn(ez, ac, __ffma2_rn(new_, as, ls.acc[i][2]));
+                ls.acc[i][3] = __ffma2_rn(ez, as, __ffma2_rn(ew, ac, ls.acc[i][3]));
+            }
         }
     }
 }
@@ -796,7 +853,7 @@ __device__ __forceinline__ int chunk_of(const int* __restrict__ begin, int n_chu
 }
 
 // Processes one (tile, ray-range) item; false if a bounded wait ran out.
-template <bool UNIFORM, bool FAST, bool FOLD>
+template <bool UNIFORM, bool FAST, bool FOLD, bool POL>
 __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, WarpShared& ws,
                              int lane) {
     // local = (sub * groups + g) * n_tiles + t: sub-range `sub` of ray group g
@@ -850,7 +907,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
             return false;
         }
         if (c != cur_chunk) {
-            if (!FOLD && cur_chunk >= 0) flush_chunk(sv, t, g, lane, ws);
+            if (!FOLD && cur_chunk >= 0) flush_chunk<POL>(sv, t, g, lane, ws);
             __syncwarp();
             if (lane == 0) {
                 const double p0x = sv.tile_center[3 * t], p0y = sv.tile_center[3 * t + 1],
@@ -870,12 +927,12 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
             setup_points<UNIFORM, FAST, FOLD>(sv, t, lane, ws, st);
             cur_chunk = c;
         }
-        prep_stage(wp.buf[b], len, lane, sv, ws);
+        prep_stage<POL>(wp.buf[b], len, lane, sv, ws);
         __syncwarp();
-        sweep_stage<UNIFORM, FOLD>(wp.buf[b], len, lane, st, ws);
+        sweep_stage<UNIFORM, FOLD, POL>(wp.buf[b], len, lane, st, ws);
         // FP32 partials run over at most kFoldStages stages of one chunk.
         if (++since_fold == kFoldStages || nlen == 0 || nc != c) {
-            fold_acc(st, ws, lane);
+            fold_acc<POL>(st, ws, lane);
             since_fold = 0;
         }
         // Order this stage's generic-proxy accesses before the next bulk
@@ -888,8 +945,8 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
         len = nlen;
         b ^= 1;
     }
-    if (FOLD) flush_item(sv, t, g, lane, ws);
-    else flush_chunk(sv, t, g, lane, ws);
+    if (FOLD) flush_item<POL>(sv, t, g, lane, ws);
+    else flush_chunk<POL>(sv, t, g, lane, ws);
     __syncwarp();
     return true;
 }
@@ -898,7 +955,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
 // sweep); solves[s].item_begin is the prefix sum of the item counts in this
 // launch, and the launch covers items [item_offset, item_offset + count) of
 // each solve.
-template <bool UNIFORM, bool FAST, bool FOLD>
+template <bool UNIFORM, bool FAST, bool FOLD, bool POL>
 __global__ void __launch_bounds__(kPrWarpsPerCta * 32, 3)
 pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long n_items,
                      unsigned long long* __restrict__ counter, int* __restrict__ err) {
@@ -933,7 +990,7 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
         }
         const PrSolve& sv = solves[lo];
         const long long local = item - sv.item_begin + sv.item_offset;
-        const bool ok = process_item<UNIFORM, FAST, FOLD>(sv, local, wp, *wsh, lane);
+        const bool ok = process_item<UNIFORM, FAST, FOLD, POL>(sv, local, wp, *wsh, lane);
         if (!ok) {
             if (lane == 0) atomicExch(err, 1);
             break;
@@ -947,14 +1004,19 @@ constexpr size_t kPrSmemBytes = (size_t)kPrWarpsPerCta * 2 * kPrStage * sizeof(P
 using PrKernel = void (*)(const PrSolve*, int, long long, unsigned long long*, int*);
 
 // Kernel of a variant: bit 0 uniform normal, bit 1 packed sweep, bit 2 folded
-// base phase (PrPlan::variant()).
-PrKernel pr_kernel(int variant) {
+// base phase, bit 3 one polarization (PrPlan::variant()).
+template <bool POL>
+PrKernel pr_kernel_pol(int v) {
     static const PrKernel table[8] = {
-        pr_persistent_kernel<false, false, false>, pr_persistent_kernel<true, false, false>,
-        pr_persistent_kernel<false, true, false>,  pr_persistent_kernel<true, true, false>,
-        pr_persistent_kernel<false, false, true>,  pr_persistent_kernel<true, false, true>,
-        pr_persistent_kernel<false, true, true>,   pr_persistent_kernel<true, true, true>};
-    return table[variant & 7];
+        pr_persistent_kernel<false, false, false, POL>, pr_persistent_kernel<true, false, false, POL>,
+        pr_persistent_kernel<false, true, false, POL>,  pr_persistent_kernel<true, true, false, POL>,
+        pr_persistent_kernel<false, false, true, POL>,  pr_persistent_kernel<true, false, true, POL>,
+        pr_persistent_kernel<false, true, true, POL>,   pr_persistent_kernel<true, true, true, POL>};
+    return table[v & 7];
+}
+
+PrKernel pr_kernel(int variant) {
+    return (variant & 8) ? pr_kernel_pol<true>(variant) : pr_kernel_pol<false>(variant);
 }
 
 // ---------------------------------------------------------------------------
@@ -1267,6 +1329,25 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             continue;
         }
         P.uniform_normal = f[11] == f[14] && f[12] == f[15] && f[13] == f[16];
+        // One common polarization (es_j, ep_j) ~ (es_0, ep_0): sum A over
+        // a_j = es_j, Ep = (ep_0 / es_0) A; with es_0 = 0 every es_j is 0 and
+        // a_j = ep_j.
+        const double a0r = f[28], a0i = f[29], b0r = f[30], b0i = f[31];
+        const bool es0 = a0r != 0.0 || a0i != 0.0, ep0 = b0r != 0.0 || b0i != 0.0;
+        P.one_pol = opt.polarization != 0 && f[27] <= kOnePolTol && (es0 || ep0);
+        if (P.one_pol && es0) {
+            const double d = a0r * a0r + a0i * a0i;
+            P.dev.amp_src = 0;
+            P.pol_es[0] = 1.0;
+            P.pol_es[1] = 0.0;
+            P.pol_ep[0] = (b0r * a0r + b0i * a0i) / d;
+            P.pol_ep[1] = (b0i * a0r - b0r * a0i) / d;
+        } else if (P.one_pol) {
+            P.dev.amp_src = 1;
+            P.pol_es[0] = P.pol_es[1] = 0.0;
+            P.pol_ep[0] = 1.0;
+            P.pol_ep[1] = 0.0;
+        }
         for (int a = 0; a < 3; ++a) {
             I.rlo[a] = f[3 + a];
             I.rhi[a] = f[6 + a];
@@ -1512,8 +1593,9 @@ Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int va
 
 Status pr_finalize(const PrPlan& P, cudaStream_t stream) {
     const int slots = P.n_tiles * kPrTile;
-    finalize_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(P.dev.partial, P.tile_perm, P.groups,
-                                                             slots, P.out);
+    finalize_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(
+        P.dev.partial, P.tile_perm, P.groups, slots, P.out, P.one_pol ? 1 : 0,
+        make_double2(P.pol_es[0], P.pol_es[1]), make_double2(P.pol_ep[0], P.pol_ep[1]));
     XK_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
 }

@@ -19,6 +19,7 @@ struct PrOptions {
     int groups = 0;               // ray groups per tile; 0 = automatic
     int sweep = -1;               // -1 automatic, 0 SFU reciprocal, 1 packed + Newton
     long long items_per_warp = 16;  // target items per resident warp (automatic groups)
+    int polarization = -1;        // -1 automatic, 0 always sum Es and Ep separately
 };
 
 // Reasons a solve is routed to the FP64 path (xk_route_reason).
@@ -56,6 +57,7 @@ struct PrSolve {
     double kt;                    // k / (2 pi), high part
     double kt_lo;                 // k / (2 pi), low part (double-double)
     float unx, uny, unz;          // the common normal (uniform-normal kernels)
+    int amp_src;                  // one-polarization kernels: 0 sum es, 1 sum ep
 };
 
 // One solve's inputs (device pointers).
@@ -74,8 +76,16 @@ struct PrPlan {
     bool uniform_normal = false;
     bool fast = false;  // packed sweep with Newton reciprocal
     bool fold = false;  // base phase folded into the per-pair phase (near field)
-    // Kernel variant: bit 0 uniform normal, bit 1 packed sweep, bit 2 folded.
-    int variant() const { return (uniform_normal ? 1 : 0) | (fast ? 2 : 0) | (fold ? 4 : 0); }
+    // Every ray's (es, ep) is a multiple of one complex pair: the kernel sums
+    // A = sum a_j U_j for one amplitude column and the field is
+    // (Es, Ep) = (pol_es, pol_ep) * A.
+    bool one_pol = false;
+    double pol_es[2] = {1.0, 0.0}, pol_ep[2] = {0.0, 0.0};
+    // Kernel variant: bit 0 uniform normal, bit 1 packed sweep, bit 2 folded,
+    // bit 3 one polarization.
+    int variant() const {
+        return (uniform_normal ? 1 : 0) | (fast ? 2 : 0) | (fold ? 4 : 0) | (one_pol ? 8 : 0);
+    }
     int n_tiles = 0, groups = 0, n_chunks = 0;
     double phase_bound = 0.0, rcp_bound = 0.0;
     PrSolve dev{};
@@ -138,7 +148,7 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
 // clear a plan's partial slots; one persistent launch over a device table of
 // solves (all of one variant) covering n_items items; a plan's final reduction.
 Status pr_zero_partials(const PrPlan& P, cudaStream_t stream);
-constexpr int kPrVariants = 8;
+constexpr int kPrVariants = 16;
 Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int variant,
                  unsigned long long* d_counter, int* d_err, cudaStream_t stream, int num_sms,
                  int max_ctas_per_sm);

@@ -69,6 +69,7 @@ class XkStats(ctypes.Structure):
         ("groups", ctypes.c_int),
         ("routed_reason", ctypes.c_int),
         ("sweep", ctypes.c_int),
+        ("one_polarization", ctypes.c_int),
     ]
 
     def to_dict(self):
@@ -94,7 +95,7 @@ class XkBatchStats(ctypes.Structure):
 class XkSolvePlan(ctypes.Structure):
     _fields_ = [("path", ctypes.c_int), ("routed_reason", ctypes.c_int), ("n_tiles", ctypes.c_int),
                 ("n_chunks", ctypes.c_int), ("groups", ctypes.c_int), ("sweep", ctypes.c_int),
-                ("phase_bound_rad", ctypes.c_double)]
+                ("phase_bound_rad", ctypes.c_double), ("one_polarization", ctypes.c_int)]
 
     def to_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
