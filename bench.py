@@ -666,6 +666,34 @@ def main():
     value = pairs * world / (ms / 1e3) / 1e9
     out32 = [t.cpu().numpy() for t in d_out]
 
+    # The same solve with Es and Ep summed separately (what any input without
+    # one common polarization runs), for comparison.
+    two_col = None
+    if stats["one_polarization"]:
+        ctx.set_option("polarization", 0)
+        solve("f32pr")
+        tms = []
+        for _ in range(3):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solve("f32pr")
+            e1.record(stream)
+            e1.synchronize()
+            tms.append(e0.elapsed_time(e1))
+        ctx.set_option("polarization", args.polarization)
+        o2 = [t.cpu().numpy() for t in d_out]
+        a = np.concatenate([out32[0] + 1j * out32[1], out32[2] + 1j * out32[3]])
+        b = np.concatenate([o2[0] + 1j * o2[1], o2[2] + 1j * o2[3]])
+        tms_mean = float(np.mean(tms))
+        if world > 1:
+            from xrt_rs import parallel
+            tms_mean = parallel.max_over_ranks(tms_mean)
+        two_col = {"value": pairs * world / (tms_mean / 1e3) / 1e9, "unit": UNIT,
+                   "ms_per_step": tms_mean, "steps": 3,
+                   "rel_l2_field_vs_one_column": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
+
     # End to end through the host C ABI: pinned host inputs -> field on host.
     e2e = None
     if not args.no_e2e:
@@ -774,7 +802,8 @@ def main():
                    "n_tiles": stats["n_tiles"], "n_chunks": stats["n_chunks"],
                    "groups": stats["groups"], "sweep": ["sfu_rcp", "packed_f32x2"][stats["sweep"]],
                    "amplitude_columns": 1 if stats["one_polarization"] else 2},
-        "e2e": e2e, "fp64_plain": fp64, "roofline": roofline, "cpu_baseline": cpu,
+        "e2e": e2e, "fp64_plain": fp64, "two_amplitude_columns": two_col,
+        "roofline": roofline, "cpu_baseline": cpu,
         "clocks": clk, "gpu_launches": launches,
     }
     if rank == 0:
