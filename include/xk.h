@@ -403,6 +403,15 @@ int xk_server_create(xk_ctx* ctx, const xk_server_opts* opts, xk_server** out);
 int xk_server_upload_rays(xk_server* server, const xk_rays* rays, size_t n, uint64_t* handle);
 int xk_server_release_rays(xk_server* server, uint64_t handle);
 
+/* A resident ray set built on the device straight from a beam: the columns of
+ * `beam`, its normals and `good` (host arrays, as xk_beam_to_rays) go to the
+ * GPU once and beam_to_diffraction_rays (src/waves/prepare_wave.rs:78-111)
+ * runs there, so the n_good ray records never exist on the host. Released
+ * with xk_server_release_rays. A good index >= n_beam returns XK_ERR_INVALID. */
+int xk_server_upload_beam(xk_server* server, const xk_beam* beam, size_t n_beam,
+                          const double* normals, const size_t* good, size_t n_good,
+                          uint64_t* handle);
+
 /* Queues a request; its host buffers must stay valid until xk_server_wait
  * returns for the ticket. Returns at once. */
 int xk_server_submit(xk_server* server, const xk_request* req, uint64_t* ticket);

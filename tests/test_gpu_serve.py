@@ -84,6 +84,34 @@ def test_resident_ray_set_serves_several_screens(ctx, oracle):
     srv.close()
 
 
+@pytest.mark.parametrize("amplitudes", [True, False])
+def test_ray_set_from_a_beam(ctx, amplitudes):
+    """xk_server_upload_beam builds the set on the device from the beam's
+    columns; requests on it equal requests carrying the same rays from the
+    host (beam_to_diffraction_rays, bit-exact) bit for bit."""
+    beam, nrm, good = cases.beam_case(6000, seed=8, amplitudes=amplitudes)
+    rays = xrt_rs.beam_to_diffraction_rays(beam, nrm, good, ctx=ctx)
+    screens = [synth.grid_screen(17, 13, 0.3, 2000.0), synth.line_screen(101, 0.4, 2500.0)]
+    for scr in screens:
+        scr["y"], scr["z"] = scr["z"].copy(), scr["y"].copy()  # the beam runs along +y
+    srv = Server(ctx)
+    before = srv.stats()["resident_ray_bytes"]
+    h = srv.upload_beam(beam, nrm, good)
+    assert srv.stats()["resident_ray_bytes"] - before == 96 * len(good)
+    for scr in screens:
+        a = srv.wait(srv.submit(scr, rayset=h))
+        b = srv.wait(srv.submit(scr, rays=rays))
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+        assert np.linalg.norm(a[0]) > 0
+    srv.release_rays(h)
+    assert srv.stats()["resident_ray_bytes"] == before
+    with pytest.raises(xrt_rs.XkError) as ei:
+        srv.upload_beam(beam, nrm, np.array([0, len(beam["x"])], dtype=np.uint64))
+    assert ei.value.code == xrt_rs._lib.XK_ERR_INVALID
+    srv.close()
+
+
 def test_budget_queues_and_rejects(ctx, oracle):
     reqs = small_requests(seed=12, count=5)
     one = max(len(r["x"]) for r, _ in reqs)

@@ -745,6 +745,85 @@ int xk_server_upload_rays(xk_server* s, const xk_rays* rays, size_t n, uint64_t*
     return XK_OK;
 }
 
+int xk_server_upload_beam(xk_server* s, const xk_beam* beam, size_t n_beam,
+                          const double* normals, const size_t* good, size_t n_good,
+                          uint64_t* handle) {
+    if (!s || !beam || !normals || !good || !handle || n_good == 0) return XK_ERR_INVALID;
+    if (!beam->x || !beam->y || !beam->z || !beam->a || !beam->b || !beam->c || !beam->e)
+        return XK_ERR_INVALID;
+    const int amps = !!beam->es_re + !!beam->es_im + !!beam->ep_re + !!beam->ep_im;
+    if (amps != 0 && amps != 4) return XK_ERR_INVALID;
+    // beam_to_diffraction_rays indexes the beam with `good` (the reference
+    // panics on an index out of range).
+    for (size_t i = 0; i < n_good; ++i)
+        if (good[i] >= n_beam) return XK_ERR_INVALID;
+    static_assert(sizeof(size_t) == sizeof(uint64_t), "good indices are copied as 64-bit words");
+    const double bytes = 96.0 * (double)n_good;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->used_bytes + bytes > s->opts.hbm_budget_bytes) return XK_ERR_BUDGET;
+        s->used_bytes += bytes;
+        s->ray_bytes += bytes;
+        s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
+    }
+    cudaSetDevice(s->ctx->device);
+    RaySet* rs = new RaySet();
+    rs->n = n_good;
+    cudaStream_t st = s->io_stream;
+    rs->buf.async_stream = st;
+    // The beam's columns, normals and indices are staged in a transient
+    // stream-ordered allocation, gathered into the set's 12 columns by
+    // beam_rays_kernel (xk_wave.cu) and freed before the call returns.
+    xk::DevBuf stage;
+    stage.async_stream = st;
+    const int cols = amps ? 11 : 7;
+    const size_t nb = n_beam * sizeof(double);
+    xk::Status stt = rs->buf.ensure(12 * n_good * sizeof(double));
+    if (stt.ok()) stt = stage.ensure((size_t)(cols + 3) * nb + n_good * sizeof(uint64_t));
+    xk::BeamDev bd{};
+    const uint64_t* d_good = nullptr;
+    if (stt.ok()) {
+        const double* src[11] = {beam->x, beam->y, beam->z, beam->a, beam->b, beam->c, beam->e,
+                                 beam->es_re, beam->es_im, beam->ep_re, beam->ep_im};
+        const double** dst = reinterpret_cast<const double**>(&bd);
+        double* d = stage.as<double>();
+        for (int f = 0; f < cols && stt.ok(); ++f, d += n_beam) {
+            dst[f] = d;
+            stt = xk::Status::FromCuda(cudaMemcpyAsync(d, src[f], nb, cudaMemcpyHostToDevice, st));
+        }
+        bd.normals = d;
+        if (stt.ok())
+            stt = xk::Status::FromCuda(
+                cudaMemcpyAsync(d, normals, 3 * nb, cudaMemcpyHostToDevice, st));
+        d_good = reinterpret_cast<const uint64_t*>(d + 3 * n_beam);
+        if (stt.ok())
+            stt = xk::Status::FromCuda(cudaMemcpyAsync(const_cast<uint64_t*>(d_good), good,
+                                                       n_good * sizeof(uint64_t),
+                                                       cudaMemcpyHostToDevice, st));
+    }
+    if (stt.ok()) {
+        double* out[12];
+        for (int f = 0; f < 12; ++f) out[f] = rs->buf.as<double>() + (size_t)f * n_good;
+        stt = xk::beam_rays_enqueue(bd, d_good, n_good, out, st);
+    }
+    stage.release();
+    // Requests that use the set are planned on other streams: the set must be
+    // complete before this call returns.
+    const cudaError_t se = cudaStreamSynchronize(st);
+    if (stt.ok() && se != cudaSuccess) stt = xk::Status::FromCuda(se);
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (!stt.ok()) {
+        s->used_bytes -= bytes;
+        s->ray_bytes -= bytes;
+        rs->buf.release();
+        delete rs;
+        return stt.code;
+    }
+    *handle = s->next_rayset++;
+    s->raysets[*handle] = rs;
+    return XK_OK;
+}
+
 int xk_server_release_rays(xk_server* s, uint64_t handle) {
     if (!s) return XK_ERR_INVALID;
     std::lock_guard<std::mutex> lock(s->mu);

@@ -208,6 +208,9 @@ _SIGNATURES = {
     "xk_server_upload_rays": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkRays),
                                               ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]),
     "xk_server_release_rays": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "xk_server_upload_beam": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.POINTER(XkBeam), ctypes.c_size_t, _dp,
+        ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]),
     "xk_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkRequest),
                                          ctypes.POINTER(ctypes.c_uint64)]),
     "xk_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,

@@ -56,6 +56,19 @@ class Server:
         self._sets[h.value] = r
         return h.value
 
+    def upload_beam(self, beam, normals, good) -> int:
+        """A resident ray set made on the device from a beam's columns
+        (beam_to_diffraction_rays of ``good``; arguments as
+        ``xrt_rs.beam_to_diffraction_rays``). Returns its handle."""
+        from .waves import _beam_args
+        xb, n, nrm, g, keep = _beam_args(beam, normals, good)
+        h = ctypes.c_uint64()
+        gp = g.ctypes.data_as(ctypes.POINTER(ctypes.c_size_t))
+        _lib.check(_lib.load().xk_server_upload_beam(self._h, ctypes.byref(xb), n, _ptr(nrm), gp,
+                                                     len(g), ctypes.byref(h)))
+        del keep
+        return h.value
+
     def release_rays(self, handle: int):
         _lib.check(_lib.load().xk_server_release_rays(self._h, handle))
         self._sets.pop(handle, None)
