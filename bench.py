@@ -446,7 +446,7 @@ def run_fresnel(args):
                         "ms_per_step": st64["gpu_ms"],
                         "speedup_separable_vs_f64": st64["gpu_ms"] / dev,
                         "rel_l2_separable_vs_f64": err},
-        "roofline": {"bound": "tensor", "kernel": "fresnel_gemm_kernel",
+        "roofline": {"bound": "tensor", "kernel": "fresnel_fused_kernel",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": None, "kernel_ms": gemm,
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst; f16 runs at the "

@@ -157,14 +157,27 @@ __device__ __forceinline__ float round_nearest(float x) {
     return __fsub_rn(__fadd_rn(x, kMagic), kMagic);
 }
 
-__device__ __forceinline__ float pair_turns(float kh, float kl, float pr, float rh, float rl) {
-    const float p1 = __fmul_rn(kh, rh);
-    const float e1 = __fmaf_rn(kh, rh, -p1);
-    const float f1 = __fsub_rn(p1, round_nearest(p1));
-    float sm = __fmaf_rn(kh, rl, e1);
-    sm = __fmaf_rn(kl, rh, sm);
-    const float t = __fadd_rn(__fadd_rn(pr, f1), sm);
-    return __fsub_rn(t, round_nearest(t));
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// The same for a row of A (.x) and a row of B (.y) at once on sm_100's packed
+// f32x2 instructions, with the operation sequence and roundings of the scalar
+// form: p1 = kh rh rounded, e1 = its FMA error, f1 = p1 - rint(p1),
+// t = (pr + f1) + (kh rl + kl rh + e1), result t - rint(t). rint is the
+// magic-number rounding (exact and sign-symmetric for |x| < 2^22), and the
+// product is carried negated (khn = -kh) so that every step is one packed
+// FMA, multiply or add; a - b is formed as fma(b, -1, a).
+__device__ __forceinline__ float2 pair_turns2(float2 kh, float2 khn, float2 kl, float2 pr,
+                                              float2 rh, float2 rl) {
+    const float2 m = f2(kMagic), mn = f2(-kMagic), one_n = f2(-1.f);
+    const float2 p1n = __fmul2_rn(khn, rh);                          // -p1
+    const float2 e1 = __ffma2_rn(kh, rh, p1n);                       // kh rh - p1
+    const float2 r1 = __fadd2_rn(__fadd2_rn(p1n, m), mn);            // rint(-p1)
+    const float2 f1n = __ffma2_rn(r1, one_n, p1n);                   // -f1
+    float2 sm = __ffma2_rn(kh, rl, e1);
+    sm = __ffma2_rn(kl, rh, sm);
+    const float2 t = __fadd2_rn(__ffma2_rn(f1n, one_n, pr), sm);    // (pr + f1) + sm
+    const float2 rt = __fadd2_rn(__fadd2_rn(t, m), mn);
+    return __ffma2_rn(rt, one_n, t);                                 // t - rint(t)
 }
 
 // hi/lo float split of a double and frac(a v^2) as a float.
@@ -179,7 +192,8 @@ __device__ __forceinline__ void split_coord(double v, double a, float* hi, float
 __device__ __forceinline__ void split16x2(float a, float b, uint32_t* hi, uint32_t* lo) {
     const __half2 h = __floats2half2_rn(a, b);
     const float2 back = __half22float2(h);
-    const __half2 l = __floats2half2_rn(a - back.x, b - back.y);
+    const float2 d = __ffma2_rn(back, f2(-1.f), make_float2(a, b));
+    const __half2 l = __floats2half2_rn(d.x, d.y);
     *hi = *reinterpret_cast<const uint32_t*>(&h);
     *lo = *reinterpret_cast<const uint32_t*>(&l);
 }
@@ -335,8 +349,12 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             split_coord(zr, g.a_turns, &h0, &l0, &pz);
             split_coord(xr, g.a_turns, &h0, &l0, &px);
         }
+        const float2 kh2 = make_float2(kzh, kxh), khn2 = make_float2(-kzh, -kxh),
+                     kl2 = make_float2(kzl, kxl), pp2 = make_float2(pz, px);
         auto stage = [&](int buf) { return reinterpret_cast<float4*>(rays_smem + buf * kFRayBytes); };
-        // Ray values of block `blk` (threads 0..31, one ray each).
+        // Ray values of block `blk` (threads 0..31, one ray each), laid out
+        // as (z, x) pairs for the packed phase: {zh, xh, zl, xl},
+        // {zf, xf, es_re, es_im} (amplitude scaled).
         auto fetch = [&](int blk, float4* v0, float4* v1) {
             const size_t j = (size_t)(rb0 + blk) * kFRays + p;
             if (p >= 32) return;
@@ -348,8 +366,8 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             float xh, xl, xf, zh, zl, zf;
             split_coord(__ldg(g.rx + j) - g.ox, g.a_turns, &xh, &xl, &xf);
             split_coord(__ldg(g.rz + j) - g.oz, g.a_turns, &zh, &zl, &zf);
-            *v0 = make_float4(xh, xl, xf, zh);
-            *v1 = make_float4(zl, zf, (float)(__ldg(g.er + j) * g.inv_scale),
+            *v0 = make_float4(zh, xh, zl, xl);
+            *v1 = make_float4(zf, xf, (float)(__ldg(g.er + j) * g.inv_scale),
                               (float)(__ldg(g.ei + j) * g.inv_scale));
         };
         auto put = [&](int buf, float4 v0, float4 v1) {
@@ -379,15 +397,16 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
                 for (int jj = 0; jj < 4; ++jj) {
                     const int j = 4 * c + jj;
                     const float4 v0 = sr[2 * j], v1 = sr[2 * j + 1];
-                    float ca = 0.f, sa = 0.f, wr = 0.f, wi = 0.f;
-                    if (va) {
-                        const float t = pair_turns(kzh, kzl, __fadd_rn(pz, v1.y), v0.w, v1.x);
-                        __sincosf(6.28318530717958647692f * t, &sa, &ca);
-                    }
+                    // Phase in turns of the A row (.x) and the B row (.y).
+                    const float2 t = pair_turns2(kh2, khn2, kl2,
+                                                 __fadd2_rn(pp2, make_float2(v1.x, v1.y)),
+                                                 make_float2(v0.x, v0.y), make_float2(v0.z, v0.w));
+                    const float2 th = __fmul2_rn(t, f2(6.28318530717958647692f));
+                    float ca, sa, cb, sb, wr = 0.f, wi = 0.f;
+                    __sincosf(th.x, &sa, &ca);
+                    __sincosf(th.y, &sb, &cb);
+                    if (!va) ca = sa = 0.f;
                     if (vb) {
-                        float cb, sb;
-                        const float t = pair_turns(kxh, kxl, __fadd_rn(px, v0.z), v0.x, v0.y);
-                        __sincosf(6.28318530717958647692f * t, &sb, &cb);
                         wr = v1.z * cb - v1.w * sb;
                         wi = v1.z * sb + v1.w * cb;
                     }
