@@ -352,40 +352,43 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
         const float2 kh2 = make_float2(kzh, kxh), khn2 = make_float2(-kzh, -kxh),
                      kl2 = make_float2(kzl, kxl), pp2 = make_float2(pz, px);
         auto stage = [&](int buf) { return reinterpret_cast<float4*>(rays_smem + buf * kFRayBytes); };
-        // Ray values of block `blk` (threads 0..31, one ray each), laid out
-        // as (z, x) pairs for the packed phase: {zh, xh, zl, xl},
-        // {zf, xf, es_re, es_im} (amplitude scaled).
-        auto fetch = [&](int blk, float4* v0, float4* v1) {
+        // Ray values of block `blk` (threads 0..31, one ray each). `fetch`
+        // only issues the loads, so that they are in flight during the
+        // block's phasors; `put` splits them and stages them as (z, x) pairs
+        // for the packed phase: {zh, xh, zl, xl}, {zf, xf, es_re, es_im}
+        // (amplitude scaled).
+        struct RawRay {
+            double x, z, er, ei;
+        };
+        auto fetch = [&](int blk, RawRay* v) {
             const size_t j = (size_t)(rb0 + blk) * kFRays + p;
             if (p >= 32) return;
             if (j >= g.n) {
-                *v0 = make_float4(0.f, 0.f, 0.f, 0.f);
-                *v1 = make_float4(0.f, 0.f, 0.f, 0.f);
+                *v = RawRay{g.ox, g.oz, 0.0, 0.0};
                 return;
             }
-            float xh, xl, xf, zh, zl, zf;
-            split_coord(__ldg(g.rx + j) - g.ox, g.a_turns, &xh, &xl, &xf);
-            split_coord(__ldg(g.rz + j) - g.oz, g.a_turns, &zh, &zl, &zf);
-            *v0 = make_float4(zh, xh, zl, xl);
-            *v1 = make_float4(zf, xf, (float)(__ldg(g.er + j) * g.inv_scale),
-                              (float)(__ldg(g.ei + j) * g.inv_scale));
+            *v = RawRay{__ldg(g.rx + j), __ldg(g.rz + j), __ldg(g.er + j), __ldg(g.ei + j)};
         };
-        auto put = [&](int buf, float4 v0, float4 v1) {
+        auto put = [&](int buf, const RawRay& v) {
             if (p < 32) {
-                stage(buf)[2 * p] = v0;
-                stage(buf)[2 * p + 1] = v1;
+                float xh, xl, xf, zh, zl, zf;
+                split_coord(v.x - g.ox, g.a_turns, &xh, &xl, &xf);
+                split_coord(v.z - g.oz, g.a_turns, &zh, &zl, &zf);
+                stage(buf)[2 * p] = make_float4(zh, xh, zl, xl);
+                stage(buf)[2 * p + 1] = make_float4(zf, xf, (float)(v.er * g.inv_scale),
+                                                    (float)(v.ei * g.inv_scale));
             }
         };
         if (nrb > 0) {
-            float4 v0, v1;
-            fetch(0, &v0, &v1);
-            put(0, v0, v1);
+            RawRay v;
+            fetch(0, &v);
+            put(0, v);
         }
         producer_sync();
         for (int i = 0; i < nrb; ++i) {
             const int s = i % kFStages, rbuf = i & 1;
-            float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0;
-            if (i + 1 < nrb) fetch(i + 1, &n0, &n1);  // in flight during this block
+            RawRay nxt{g.ox, g.oz, 0.0, 0.0};
+            if (i + 1 < nrb) fetch(i + 1, &nxt);  // in flight during this block
             if (!mbar_wait(&empty[s], ((uint32_t)(i / kFStages) & 1u) ^ 1u)) *flag = 1;
             unsigned char* base = tiles + (size_t)s * kFStage;
             const float4* sr = stage(rbuf);
@@ -438,7 +441,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&full[s]);
-            if (i + 1 < nrb) put(rbuf ^ 1, n0, n1);
+            if (i + 1 < nrb) put(rbuf ^ 1, nxt);
             producer_sync();
         }
     }
