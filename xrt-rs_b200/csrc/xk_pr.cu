@@ -784,10 +784,11 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
     constexpr int H = kPrPpl / 2;
     const float4* rec = reinterpret_cast<const float4*>(buf);
     // Two rays per iteration give the scheduler two independent sets of
-    // chains (+3 % one-column, +1 % two-column on the far-field workload);
-    // the general-normal two-column kernels are at the register limit of
-    // three CTAs per SM and keep one.
-#pragma unroll ((UNIFORM || POL) ? 2 : 1)
+    // chains (+3 % one-column, +1 % two-column on the far-field workload).
+    // The folded (near-field) kernels switch chunks every few stages and ran
+    // ~5 % slower unrolled; they and the general-normal two-column kernels,
+    // which are at the register limit of three CTAs per SM, keep one.
+#pragma unroll (((UNIFORM || POL) && !FOLD) ? 2 : 1)
     for (int j = 0; j < len; ++j) {
         const float4 a = rec[4 * j + 0];
         const float4 b = rec[4 * j + 1];
