@@ -174,6 +174,12 @@ def cpu_baseline(rays, screen, seconds: float):
                       f"OpenMP over screen points)"}
 
 
+def single_workload(n_rays: int, grid: int) -> str:
+    """Name of the single-solve workload (both arms)."""
+    return (f"single solve: {n_rays} rays (Gaussian aperture sigma 0.1 mm, 10 keV) x "
+            f"{grid}x{grid} screen +-0.5 mm at 1000 mm")
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -211,8 +217,11 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"single solve, {args.rays} rays x {args.grid}x{args.grid} screen "
-                               "(CPU sample)", "rays": args.rays, "screen": args.grid ** 2},
+        "config": {"workload": single_workload(args.rays, args.grid), "rays": args.rays,
+                   "screen_points": args.grid ** 2,
+                   "pairs_per_step": float(args.rays) * float(args.grid ** 2),
+                   "parallelism": "rank 0 only (host cores)",
+                   "timed_sample_pairs_per_step": float(pairs)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -799,8 +808,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"single solve: {n} rays (Gaussian aperture sigma 0.1 mm, 10 keV) x "
-                               f"{args.grid}x{args.grid} screen +-0.5 mm at 1000 mm",
+        "config": {"workload": single_workload(n, args.grid),
                    "rays": n, "screen_points": m, "pairs_per_step": pairs,
                    "parallelism": f"replica x{world}", "l2": "flushed between steps (256 MiB write)",
                    "path": "f32pr", "phase_bound_rad": stats["phase_bound_rad"],
