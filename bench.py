@@ -219,9 +219,9 @@ def run_reference(args):
         "data": "synthetic",
         "config": {"workload": single_workload(args.rays, args.grid), "rays": args.rays,
                    "screen_points": args.grid ** 2,
-                   "pairs_per_step": float(args.rays) * float(args.grid ** 2),
+                   "workload_pairs": float(args.rays) * float(args.grid ** 2),
                    "parallelism": "rank 0 only (host cores)",
-                   "timed_sample_pairs_per_step": float(pairs)},
+                   "pairs_per_step": float(pairs)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
