@@ -457,6 +457,45 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
 
 // acc[iz*nx + ix] (+)= scale * sum over splits of C[iz][2ix + c], in FP64 and
 // split order.
+// The ray set's bounds the product needs before it starts: max |es_re|,
+// |es_im| (the f16 scaling), max |x - ox| and |z - oz| (the cross-term bound),
+// and whether every value is finite. The maxima of non-negative doubles are
+// taken on their bit patterns, which order like the values; fmax skips NaN,
+// which the finiteness flag reports instead.
+__global__ void __launch_bounds__(256) ray_bounds_kernel(const double* __restrict__ rx,
+                                                         const double* __restrict__ rz,
+                                                         const double* __restrict__ er,
+                                                         const double* __restrict__ ei, size_t n,
+                                                         double ox, double oz,
+                                                         unsigned long long* __restrict__ max_bits,
+                                                         int* __restrict__ nonfinite) {
+    double m[3] = {0.0, 0.0, 0.0};
+    bool bad = false;
+    for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n;
+         j += (size_t)gridDim.x * blockDim.x) {
+        const double x = rx[j], z = rz[j], a = er[j], b = ei[j];
+        m[0] = fmax(m[0], fmax(fabs(a), fabs(b)));
+        m[1] = fmax(m[1], fabs(x - ox));
+        m[2] = fmax(m[2], fabs(z - oz));
+        bad = bad || !isfinite(x + z + a + b);
+    }
+    __shared__ double sm[8][3];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double v = m[k];
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) sm[warp][k] = v;
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicExch(nonfinite, 1);
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = sm[0][threadIdx.x];
+        for (int w = 1; w < 8; ++w) v = fmax(v, sm[w][threadIdx.x]);
+        atomicMax(max_bits + threadIdx.x, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
 __global__ void reduce_kernel(const double* __restrict__ partial, int splits, int m_pad, int n_pad,
                               size_t nz, size_t nx, double scale, double* __restrict__ acc_re,
                               double* __restrict__ acc_im, int first) {
@@ -617,12 +656,34 @@ xk::Status fresnel_host(xk_ctx* ctx, const double* rx, const double* rz, const d
     double max_amp = 0.0, max_rx = 0.0, max_rz = 0.0;
     const double ox = 0.5 * (sc->x_min + sc->x_max), oz = 0.5 * (sc->z_min + sc->z_max);
     bool finite = true;
-    for (size_t j = 0; j < n; ++j) {
+    int bounds_kernels = 0;
+    if (n) {
+        // The bounds come from the uploaded columns on the device (a host
+        // loop over 2^20 rays takes milliseconds); one small read-back.
+        XK_TRY(ws.ctrl.ensure(256));
+        unsigned long long* d_max = reinterpret_cast<unsigned long long*>(ws.ctrl.as<char>() + 64);
+        int* d_bad = reinterpret_cast<int*>(d_max + 3);
+        XK_CUDA_TRY(cudaMemsetAsync(d_max, 0, 3 * sizeof(unsigned long long) + sizeof(int), s));
+        const unsigned blocks =
+            (unsigned)std::min<size_t>((n + 255) / 256, (size_t)std::max(ctx->num_sms, 1) * 4);
+        xk::ray_bounds_kernel<<<blocks, 256, 0, s>>>(d, d + n, d + 2 * n, d + 3 * n, n, ox, oz,
+                                                     d_max, d_bad);
+        XK_CUDA_TRY(cudaGetLastError());
+        bounds_kernels = 1;
+        struct {
+            unsigned long long m[3];
+            int bad;
+        } h{};
+        XK_CUDA_TRY(cudaMemcpyAsync(&h, d_max, sizeof(h.m) + sizeof(int),
+                                    cudaMemcpyDeviceToHost, s));
+        XK_CUDA_TRY(cudaStreamSynchronize(s));
+        double v[3];
+        std::memcpy(v, h.m, sizeof(v));
         // An upper bound of |es_j| is all the f16 scaling needs.
-        max_amp = std::max(max_amp, std::max(std::fabs(er[j]), std::fabs(ei[j])));
-        max_rx = std::max(max_rx, std::fabs(rx[j] - ox));
-        max_rz = std::max(max_rz, std::fabs(rz[j] - oz));
-        finite = finite && std::isfinite(rx[j] + rz[j] + er[j] + ei[j]);
+        max_amp = v[0];
+        max_rx = v[1];
+        max_rz = v[2];
+        finite = h.bad == 0;
     }
     max_amp *= 1.4142135623730951;
     double* out = ctx->out_field.as<double>();
@@ -669,7 +730,7 @@ xk::Status fresnel_host(xk_ctx* ctx, const double* rx, const double* rz, const d
         XK_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         stats->gpu_ms = ms;
         stats->main_kernel_ms = rep.gemm_ms;
-        stats->kernels = rep.kernels;
+        stats->kernels = rep.kernels + bounds_kernels;
         stats->path = rep.used_path;
         stats->pairs = (double)n * (double)m;
         stats->h2d_bytes = 4.0 * nb;
