@@ -1,0 +1,58 @@
+"""bench.py --impl reference on the CPU: the timed CPU algorithm of the path
+(the oracle port), one JSON line on the same workload, metric and unit as the
+CUDA arm; under torchrun only rank 0 works and prints, the other ranks exit 0.
+"""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ARGS = ["--impl", "reference", "--steps", "1", "--warmup", "1", "--rays", "4096", "--grid", "64"]
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _json_lines(out):
+    return [json.loads(l) for l in out.splitlines() if l.startswith("{")]
+
+
+def _check(line):
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["impl"] == "reference"
+    assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["higher_is_better"] is True
+    assert line["config"]["workload"] == bench.single_workload(4096, 64)
+    assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_single_process():
+    r = subprocess.run([sys.executable, "bench.py", *ARGS], cwd=ROOT, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _json_lines(r.stdout)
+    assert len(lines) == 1
+    _check(lines[0])
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), "bench.py",
+           "--gpus", "2", *ARGS]
+    env = dict(os.environ, OMP_NUM_THREADS="2")
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300, env=env)
+    if r.returncode != 0 and "torch.distributed" in r.stderr and "No module" in r.stderr:
+        pytest.skip("torch.distributed.run unavailable")
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _json_lines(r.stdout)
+    assert len(lines) == 1
+    _check(lines[0])
