@@ -153,10 +153,6 @@ __device__ __forceinline__ uint32_t sw128(uint32_t r, uint32_t c) {
 // part drops out and the fractional remainder keeps ~1e-7 turn.
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: (x + kMagic) - kMagic = rint(x), |x| < 2^22
 
-__device__ __forceinline__ float round_nearest(float x) {
-    return __fsub_rn(__fadd_rn(x, kMagic), kMagic);
-}
-
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
 // The same for a row of A (.x) and a row of B (.y) at once on sm_100's packed
@@ -422,19 +418,20 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
                     make_uint4(al[0], al[1], al[2], al[3]);
                 unsigned char* bhi = base + 2 * kFA;
                 unsigned char* blo = bhi + kFB;
-                // Rows 2r and 2r+1, the first store to row 2r + sel: eight
-                // consecutive threads then hit eight distinct swizzle phases.
-                const int sel = (r >> 2) & 1;
+                // Rows 2r and 2r+1. Eight consecutive threads' stores to even
+                // rows meet four swizzle phases (a 2-way conflict); ordering
+                // the two stores per thread to spread them cost 16 selects
+                // per chunk and was 1.5 % slower overall.
                 const uint4 e0h = make_uint4(neg_hi(bh[0]), neg_hi(bh[1]), neg_hi(bh[2]), neg_hi(bh[3]));
                 const uint4 e1h = make_uint4(swap_halves(bh[0]), swap_halves(bh[1]),
                                              swap_halves(bh[2]), swap_halves(bh[3]));
                 const uint4 e0l = make_uint4(neg_hi(bl[0]), neg_hi(bl[1]), neg_hi(bl[2]), neg_hi(bl[3]));
                 const uint4 e1l = make_uint4(swap_halves(bl[0]), swap_halves(bl[1]),
                                              swap_halves(bl[2]), swap_halves(bl[3]));
-                *reinterpret_cast<uint4*>(bhi + sw128(2 * r + sel, c)) = sel ? e1h : e0h;
-                *reinterpret_cast<uint4*>(bhi + sw128(2 * r + 1 - sel, c)) = sel ? e0h : e1h;
-                *reinterpret_cast<uint4*>(blo + sw128(2 * r + sel, c)) = sel ? e1l : e0l;
-                *reinterpret_cast<uint4*>(blo + sw128(2 * r + 1 - sel, c)) = sel ? e0l : e1l;
+                *reinterpret_cast<uint4*>(bhi + sw128(2 * r, c)) = e0h;
+                *reinterpret_cast<uint4*>(bhi + sw128(2 * r + 1, c)) = e1h;
+                *reinterpret_cast<uint4*>(blo + sw128(2 * r, c)) = e0l;
+                *reinterpret_cast<uint4*>(blo + sw128(2 * r + 1, c)) = e1l;
             }
             // Make the generic-proxy stores visible to the tensor cores, then
             // one arrival per warp.
