@@ -434,6 +434,10 @@ def run_fresnel(args):
                        "this pool (MEASURED_PEAKS.json absent; f16 runs at the bf16 rate)")
     gemm = float(np.mean(gemm_ms))
     achieved = algo_flops / (gemm / 1e3) / 1e12
+    # DRAM bytes (read + write) of one fresnel_fused_kernel launch on the
+    # 2^20-ray 512x512 workload, from a single-pass ncu capture of full-size
+    # launches (profiles/fresnel_fused_2p16x256sq_ncu.md); other sizes null.
+    fr_traffic = 33.8e6 if (args.rays == 1 << 20 and args.grid == 512) else None
     cpu = None
     if not args.no_cpu:
         row = xrt_rs.FresnelScreen(-0.5, 0.5, g, 0.0, 0.0, 1)
@@ -463,7 +467,7 @@ def run_fresnel(args):
                         "rel_l2_separable_vs_f64": err},
         "roofline": {"bound": "tensor", "kernel": "fresnel_fused_kernel",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": None, "kernel_ms": gemm,
+                     "traffic": fr_traffic, "kernel_ms": gemm,
                      "peak_source": peak_source,
                      "algorithmic_flops": algo_flops},
         "cpu_baseline": cpu, "clocks": clk,
