@@ -42,7 +42,8 @@ def test_version_and_status_strings():
     assert xrt_rs.route_reason(0) == ""
     assert xrt_rs.route_reason(1) == "no rays"
     assert xrt_rs.route_reason(7) == "non-finite ray or screen values"
-    assert xrt_rs.route_reason(8) == "unknown"
+    assert xrt_rs.route_reason(8) == "amplitudes outside the FP32 range of the phase-reduced sums"
+    assert xrt_rs.route_reason(9) == "unknown"
 
 
 def test_length_mismatch_raises_value_error():

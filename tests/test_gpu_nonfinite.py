@@ -135,3 +135,30 @@ def test_fresnel_all_zero_amplitudes_but_one_nan(ctx):
     res, st = xrt_rs.fresnel_propagate(x, z, es, 10000.0, 1000.0, sc, ctx=ctx, return_stats=True)
     assert st["path"] == xrt_rs.XK_PATH_F64
     assert np.isnan(res.amplitude).all()
+
+
+AMP_RANGE_REASON = 8
+
+
+@pytest.mark.parametrize("scale,routed", [(1e-35, True), (1e35, True), (1e-25, False),
+                                          (1e25, False)])
+def test_amplitude_range(ctx, oracle, scale, routed):
+    """Amplitudes the FP32 sums cannot carry (beyond 1e30 or below 1e-30 in
+    every component) take the FP64 sum; inside that range the phase-reduced
+    result scales with them."""
+    rays, pix = synth.config0(seed=6)
+    rays = {k: np.array(v, dtype=np.float64) for k, v in rays.items()}
+    base = xrt_rs.diffraction_integral(*cases.as_lists(rays, pix), path="f32pr", ctx=ctx)
+    for k in ("es_re", "es_im", "ep_re", "ep_im"):
+        rays[k] = rays[k] * scale
+    lists = cases.as_lists(rays, pix)
+    out, st = xrt_rs.diffraction_integral(*lists, path="f32pr", ctx=ctx, return_stats=True)
+    if routed:
+        assert st["path"] == xrt_rs.XK_PATH_F64 and st["routed_reason"] == AMP_RANGE_REASON
+        ref = oracle.kahan_f64(*lists)
+        assert cases.rel_l2(out, ref) < 1e-10
+    else:
+        assert st["path"] == xrt_rs.XK_PATH_F32PR
+        scaled = [np.asarray(b) * scale for b in base]
+        assert cases.rel_l2(out, scaled) < 1e-6
+

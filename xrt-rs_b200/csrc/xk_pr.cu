@@ -54,7 +54,7 @@ namespace xk {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kSumFields = 32;
+constexpr int kSumFields = 33;
 // Stages of FP32 partial sums per fold into the two-float accumulators.
 constexpr int kFoldStages = 1;
 // |e| bound under which the packed sweep's series reciprocal is used.
@@ -66,6 +66,10 @@ constexpr double kFoldChunksPerGroup = 4.0;
 // the per-ray deviation is then below the FP32 rounding of the amplitudes
 // that the kernel applies anyway).
 constexpr double kOnePolTol = 5.9604644775390625e-8;
+// Amplitude components the phase-reduced kernels carry in FP32: their partial
+// sums over a chunk (up to 2^20 rays, |U| up to ~1/path) must stay inside
+// FP32's range, and products with |U| must stay normal.
+constexpr double kF32AmpMax = 1e30, kF32AmpMin = 1e-30;
 
 // ---------------------------------------------------------------------------
 // Planner kernels
@@ -81,9 +85,10 @@ __constant__ int c_sum_ops[kSumFields] = {
     OP_MIN, OP_MIN, OP_MIN, OP_MAX, OP_MAX, OP_MAX,  // screen bbox
     OP_SUM,                                          // non-finite probe
     OP_MAX,                                          // polarization deviation
-    OP_SUM, OP_SUM, OP_SUM, OP_SUM};                 // ray 0's es, ep
-const int h_sum_ops[kSumFields] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 1, 2, 1, 1, 1, 2, 2,
-                                   2, 0, 0, 0, 1, 1, 1, 2, 2, 2, 0, 2, 0, 0, 0, 0};
+    OP_SUM, OP_SUM, OP_SUM, OP_SUM,                  // ray 0's es, ep
+    OP_MAX};                                         // largest amplitude component
+const int h_sum_ops[kSumFields] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 1, 2, 1, 1, 1, 2, 2, 2,
+                                   0, 0, 0, 1, 1, 1, 2, 2, 2, 0, 2, 0, 0, 0, 0, 2};
 
 __device__ __forceinline__ double op_combine(int op, double a, double b) {
     return op == OP_SUM ? a + b : (op == OP_MIN ? fmin(a, b) : fmax(a, b));
@@ -93,7 +98,8 @@ __device__ __forceinline__ double op_combine(int op, double a, double b) {
 // sums every input value times zero: 0 when all are finite, NaN otherwise
 // (fmin / fmax skip NaN, so the boxes alone would not show it). Fields 27-31
 // test whether all rays share ray 0's polarization: the largest relative
-// |es_j ep_0 - ep_j es_0|, and ray 0's (es, ep).
+// |es_j ep_0 - ep_j es_0|, and ray 0's (es, ep); field 32 is the largest
+// amplitude component.
 __global__ void __launch_bounds__(256) summary_kernel(RaysDev r, int n, PixDev p, int m,
                                                      double* __restrict__ block_out) {
     double f[kSumFields];
@@ -118,6 +124,7 @@ __global__ void __launch_bounds__(256) summary_kernel(RaysDev r, int n, PixDev p
         const double nrm = sqrt(ar * ar + ai * ai) * b0n + sqrt(br * br + bi * bi) * a0n;
         const double dn = sqrt(dr * dr + di * di);
         f[27] = fmax(f[27], nrm > 0.0 ? dn / nrm : (dn > 0.0 ? INFINITY : 0.0));
+        f[32] = fmax(f[32], fmax(fmax(fabs(ar), fabs(ai)), fmax(fabs(br), fabs(bi))));
         if (i == 0) {
             f[28] += ar;
             f[29] += ai;
@@ -1180,7 +1187,8 @@ const char* const kRouteReasons[kRouteReasonCount] = {
     "ray and screen bounding boxes overlap",
     "no cell size meets the phase budget",
     "ray cell grid too fine",
-    "non-finite ray or screen values"};
+    "non-finite ray or screen values",
+    "amplitudes outside the FP32 range of the phase-reduced sums"};
 
 Status PrWorkspace::ensure_host(size_t bytes) {
     if (bytes <= host_bytes) return Status::Ok();
@@ -1322,6 +1330,11 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             P.route_reason = 7;
             continue;
         }
+        if (f[32] > kF32AmpMax || (f[32] > 0.0 && f[32] < kF32AmpMin)) {
+            P.routed = true;
+            P.route_reason = 8;
+            continue;
+        }
         if (!(f[9] == f[10])) {
             P.routed = true;
             P.route_reason = 2;
@@ -1341,12 +1354,21 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         const bool es0 = a0r != 0.0 || a0i != 0.0, ep0 = b0r != 0.0 || b0i != 0.0;
         P.one_pol = opt.polarization != 0 && f[27] <= kOnePolTol && (es0 || ep0);
         if (P.one_pol && es0) {
-            const double d = a0r * a0r + a0i * a0i;
-            P.dev.amp_src = 0;
-            P.pol_es[0] = 1.0;
-            P.pol_es[1] = 0.0;
-            P.pol_ep[0] = (b0r * a0r + b0i * a0i) / d;
-            P.pol_ep[1] = (b0i * a0r - b0r * a0i) / d;
+            // ep_0 / es_0 in extended precision (|es_0|^2 cannot underflow);
+            // a ratio beyond FP64's range keeps both columns.
+            const long double ar = a0r, ai = a0i, br = b0r, bi = b0i;
+            const long double d = ar * ar + ai * ai;
+            const double pr = (double)((br * ar + bi * ai) / d);
+            const double pi = (double)((bi * ar - br * ai) / d);
+            if (std::isfinite(pr) && std::isfinite(pi)) {
+                P.dev.amp_src = 0;
+                P.pol_es[0] = 1.0;
+                P.pol_es[1] = 0.0;
+                P.pol_ep[0] = pr;
+                P.pol_ep[1] = pi;
+            } else {
+                P.one_pol = false;
+            }
         } else if (P.one_pol) {
             P.dev.amp_src = 1;
             P.pol_es[0] = P.pol_es[1] = 0.0;

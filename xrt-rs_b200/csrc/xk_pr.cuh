@@ -23,7 +23,7 @@ struct PrOptions {
 };
 
 // Reasons a solve is routed to the FP64 path (xk_route_reason).
-constexpr int kRouteReasonCount = 8;
+constexpr int kRouteReasonCount = 9;
 extern const char* const kRouteReasons[kRouteReasonCount];
 
 // Sorted ray record as the planner writes it and TMA stages it: position
