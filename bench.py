@@ -149,6 +149,15 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def balanced_count(count: int, threads: int, limit: int) -> int:
+    """Screen points per CPU sample rounded up to a multiple of 4 x threads,
+    so that the oracle's one-point-at-a-time OpenMP schedule ends with every
+    thread busy (a sample of 92 points on 16 threads left 9 idle in its last
+    round)."""
+    unit = 4 * max(1, threads)
+    return int(min(limit, max(unit, -(-count // unit) * unit)))
+
+
 def cpu_baseline(rays, screen, seconds: float):
     """The oracle on a bounded sample of screen points, all host threads."""
     from oracle import oracle  # checker / baseline only
@@ -157,7 +166,7 @@ def cpu_baseline(rays, screen, seconds: float):
     rl = [rays[k] for k in ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re",
                             "ep_im", "energy")]
     threads = oracle.max_threads()
-    count = 8
+    count = balanced_count(8, threads, len(screen["x"]))
     rate = None
     while True:
         sub, _ = synth.subsample_screen(screen, count, seed=7)
@@ -168,6 +177,7 @@ def cpu_baseline(rays, screen, seconds: float):
         if dt >= seconds * 0.5 or count >= len(screen["x"]):
             break
         count = int(min(len(screen["x"]), max(count * 2, count * seconds * 0.6 / max(dt, 1e-3))))
+        count = balanced_count(count, threads, len(screen["x"]))
     return {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{len(rl[0])} rays x {count} seeded screen points of the workload "
                       f"({dt:.1f} s, C restatement of src/waves/diffraction.rs:56-117, "
@@ -197,6 +207,7 @@ def run_reference(args):
     oracle.kahan_f64(rl, [sub["x"], sub["y"], sub["z"]])
     per_point = (time.perf_counter() - t0) / 16
     count = int(max(16, min(len(screen["x"]), 2.0 / max(per_point, 1e-6))))
+    count = balanced_count(count, threads, len(screen["x"]))
     sub, _ = synth.subsample_screen(screen, count, seed=7)
     pl = [sub["x"], sub["y"], sub["z"]]
     for _ in range(args.warmup):

@@ -154,7 +154,16 @@ const char* xk_route_reason(int reason);
  *                    FP64 phase with the library functions, as the reference
  *                    does; 1 first reduces the phase by 2 pi with an FMA-based
  *                    Cody-Waite step (same phase value and 1e-10 parity, about
- *                    twice the throughput at phases of 1e10-1e13 rad) */
+ *                    twice the throughput at phases of 1e10-1e13 rad)
+ *   "wait_limit"     polls of every bounded device-side wait (mbarrier waits of
+ *                    the phase-reduced kernel and of the tensor-core Fresnel
+ *                    product) before the kernel gives up and the call returns
+ *                    XK_ERR_TIMEOUT; 1..2^31, default 2^24
+ *   "inject_stall"   test hook: the next phase-reduced execution on this
+ *                    context arms its first ray stage's barrier with this many
+ *                    bytes (a positive multiple of 16, at most 1024) beyond its
+ *                    copy, so that stage can never complete and the bounded
+ *                    wait runs out; cleared after that one execution */
 int xk_set_option(xk_ctx* ctx, const char* name, double value);
 
 typedef struct xk_tune_result {
@@ -435,10 +444,15 @@ void xk_server_destroy(xk_server* server);
  * No counterpart in the reference. For callers that cannot let a library
  * allocate device memory: programs whose device memory is all owned by their
  * own pool allocator, and loops that cannot pay for cudaMalloc's implicit
- * synchronisation on every call. It computes exactly what XK_PATH_F64
- * computes (same kernels), with its scratch in a fixed array inside the
- * library instead of context buffers, and it calls no cudaMalloc, cudaFree
- * or other allocating routine.
+ * synchronisation on every call. It runs the kernels of XK_PATH_F64 with
+ * its scratch in a fixed array inside the library instead of context buffers,
+ * and it calls no cudaMalloc, cudaFree or other allocating routine. Its
+ * split-ray partial sums must fit that array, so on solves of more than
+ * about 2^24 ray x screen pairs it may cut the ray list into fewer ranges
+ * than XK_PATH_F64 does (one range above 524288 screen points); the Kahan
+ * sums then run
+ * in another order, and results agree with XK_PATH_F64 to <= 1e-10 relative
+ * L2 rather than bit for bit.
  *
  * - rays, pixels and out hold DEVICE pointers on the current device; the
  *   work is enqueued on `stream` (cudaStream_t, NULL = default stream) and
@@ -448,7 +462,9 @@ void xk_server_destroy(xk_server* server);
  * - The fixed scratch is XK_NOALLOC_SCRATCH_BYTES (32 MiB) of device memory,
  *   held by every GPU on which the library's FP64 code is loaded until exit.
  * - The first call on a device looks up the scratch's device address with
- *   that device current; make that first call before any stream capture.
+ *   that device current, and so does the first call after the device's
+ *   context was replaced (cudaDeviceReset); make those calls before any
+ *   stream capture.
  * - All calls share the one scratch array and it keeps the last call's
  *   contents (every byte a call reads is written earlier in the same call, so
  *   nothing needs clearing). Calls that overlap on the GPU — from several

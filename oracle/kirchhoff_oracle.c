@@ -127,7 +127,7 @@ void oracle_kahan_f64(const double* rx, const double* ry, const double* rz,
                       double* o_ep_im, int n_threads) {
     set_threads(n_threads);
     long long m = (long long)n_pix;
-#pragma omp parallel for schedule(dynamic, 4)
+#pragma omp parallel for schedule(dynamic, 1)
     for (long long i = 0; i < m; ++i) {
         double o[4];
         kahan_pixel(rx, ry, rz, rnx, rny, rnz, rnl, es_re, es_im, ep_re, ep_im, energy,
@@ -190,7 +190,7 @@ void oracle_kahan_ld(const double* rx, const double* ry, const double* rz,
                      double* o_ep_im, int n_threads) {
     set_threads(n_threads);
     long long m = (long long)n_pix;
-#pragma omp parallel for schedule(dynamic, 4)
+#pragma omp parallel for schedule(dynamic, 1)
     for (long long i = 0; i < m; ++i) {
         double o[4];
         kahan_pixel_ld(rx, ry, rz, rnx, rny, rnz, rnl, es_re, es_im, ep_re, ep_im, energy,
@@ -210,7 +210,7 @@ void oracle_plain_f64(const double* rx, const double* ry, const double* rz,
                       double* o_ep_im, int n_threads) {
     set_threads(n_threads);
     long long m = (long long)n_pix;
-#pragma omp parallel for schedule(dynamic, 4)
+#pragma omp parallel for schedule(dynamic, 1)
     for (long long i = 0; i < m; ++i) {
         cplx es = {0.0, 0.0}, ep = {0.0, 0.0};
         for (size_t j = 0; j < n_rays; ++j) {
@@ -261,7 +261,7 @@ void oracle_wgsl_f32(const float* rx, const float* ry, const float* rz,
     float chbar_inv_1e7 = (float)(1.0 / ORACLE_CHBAR * 1e7);
     const float PI_F = 3.14159265358979323846f;
     long long m = (long long)n_pix;
-#pragma omp parallel for schedule(dynamic, 4)
+#pragma omp parallel for schedule(dynamic, 1)
     for (long long i = 0; i < m; ++i) {
         float pxi = px[i], pyi = py[i], pzi = pz[i];
         float rdx = pxi - cx, rdy = pyi - cy, rdz = pzi - cz;

@@ -1,0 +1,84 @@
+"""Device-side bounded waits run out, and the context stays usable.
+
+The failure is made on the host: the "inject_stall" test hook makes the next
+phase-reduced execution expect 16 bytes more on its first ray stage's barrier
+than the stage's bulk copy delivers. The copy lands (nothing stays in
+flight), the barrier can never complete, and the warp's bounded wait runs out
+after "wait_limit" polls. The call must return XK_ERR_TIMEOUT, and the next
+solve on the same context must be right: equal, bit for bit, to the same solve
+on a context that never failed, and within 1e-4 of the oracle. No GPU faults,
+traps or hangs: every wait involved is bounded.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import cases
+import xrt_rs
+from xrt_rs import _lib, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(ctx, rays, pix):
+    return xrt_rs.diffraction_integral(rays, pix, path="f32pr", ctx=ctx, return_stats=True)
+
+
+def test_stalled_stage_times_out_and_context_recovers(oracle):
+    rays, pix = synth.config0(seed=8)
+    rl, pl = cases.as_lists(rays, pix)
+    clean = xrt_rs.GpuContext.new(0)
+    ref_out, _ = _solve(clean, rl, pl)
+    clean.close()
+
+    ctx = xrt_rs.GpuContext.new(0)
+    try:
+        ctx.set_option("wait_limit", 4096)
+        ctx.set_option("inject_stall", 16)
+        t0 = time.perf_counter()
+        with pytest.raises(xrt_rs.XkError) as ei:
+            _solve(ctx, rl, pl)
+        dt = time.perf_counter() - t0
+        assert ei.value.code == _lib.XK_ERR_TIMEOUT, str(ei.value)
+        print(f"stalled solve returned XK_ERR_TIMEOUT after {dt * 1e3:.1f} ms: {ei.value}")
+        # The hook armed one execution only; the default limit comes back.
+        ctx.set_option("wait_limit", float(1 << 24))
+        out, st = _solve(ctx, rl, pl)
+        assert st["path"] == xrt_rs.XK_PATH_F32PR
+        for a, b in zip(out, ref_out):
+            assert np.array_equal(a, b)
+        assert cases.rel_l2(out, oracle.kahan_f64(rl, pl)) < 1e-4
+        # The FP64 path on the same context is unaffected as well.
+        out64, _ = xrt_rs.diffraction_integral(rl, pl, path="f64", ctx=ctx, return_stats=True)
+        assert cases.rel_l2(out64, oracle.kahan_f64(rl, pl)) < 1e-10
+    finally:
+        ctx.close()
+
+
+def test_wait_limit_alone_keeps_results():
+    """A lower (but sufficient) poll limit changes nothing when no stage stalls."""
+    rays, pix = synth.config0(seed=9)
+    rl, pl = cases.as_lists(rays, pix)
+    ctx = xrt_rs.GpuContext.new(0)
+    try:
+        a, _ = _solve(ctx, rl, pl)
+        ctx.set_option("wait_limit", float(1 << 20))
+        b, _ = _solve(ctx, rl, pl)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    finally:
+        ctx.close()
+
+
+def test_option_validation():
+    ctx = xrt_rs.GpuContext.new(0)
+    try:
+        for name, bad in (("wait_limit", 0), ("wait_limit", 1.5), ("wait_limit", 2.0 ** 32),
+                          ("inject_stall", 8), ("inject_stall", 2048), ("inject_stall", -16)):
+            with pytest.raises(xrt_rs.XkError) as ei:
+                ctx.set_option(name, bad)
+            assert ei.value.code == _lib.XK_ERR_INVALID
+        ctx.set_option("inject_stall", 0)  # disarms
+    finally:
+        ctx.close()

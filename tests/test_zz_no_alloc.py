@@ -72,3 +72,30 @@ def test_noalloc_rejects_more_rays_than_its_scratch_holds(ctx):
     rc, out = _noalloc(torch, _device_arrays(torch, rl), _device_arrays(torch, pl), n, 4)
     assert rc == _lib.XK_ERR_BUDGET
     assert all(np.all(o == 0) for o in out)  # nothing was launched
+
+
+@pytest.mark.parametrize("n_rays,grid,line", [
+    (2000, 256, 0),      # 2^16 screen points: the fixed area holds 8 ray ranges, the allocating path uses 19
+    (64, 0, 600_000),    # more than 2^19 screen points: no room for partials, one ray range
+])
+def test_noalloc_where_its_scratch_caps_the_ray_split(ctx, oracle, n_rays, grid, line):
+    """The two branches this entry point has of its own: fewer ray ranges than
+    the allocating path (Kahan sums in another order) and a single range.
+    Both agree with the allocating FP64 path and with the CPU oracle."""
+    torch = pytest.importorskip("torch")
+    rays, _ = cases.random_case(n_rays, 1, seed=31)
+    if grid:
+        pix = synth.grid_screen(grid, grid, 0.3, 1000.0)
+    else:
+        pix = synth.line_screen(line, 0.3, 1000.0)
+    rl, pl = cases.as_lists(rays, pix)
+    d_rays = _device_arrays(torch, rl)
+    d_pix = _device_arrays(torch, pl)
+    n, m = len(rl[0]), len(pl[0])
+    ref = _allocating(torch, ctx, d_rays, d_pix, m)
+    for _ in range(2):
+        rc, got = _noalloc(torch, d_rays, d_pix, n, m)
+        assert rc == _lib.XK_OK
+        assert cases.rel_l2(got, ref) <= F64_TOL
+    cpu = oracle.kahan_f64(rl, pl)
+    assert cases.rel_l2(got, cpu) <= F64_TOL

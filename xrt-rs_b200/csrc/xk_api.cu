@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -331,6 +332,15 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
     } else if (n == "items_per_warp") {
         if (value < 1.0 || value > 4096.0) return fail(ctx, XK_ERR_INVALID, "items_per_warp out of range");
         ctx->pr_opts.items_per_warp = (long long)value;
+    } else if (n == "wait_limit") {
+        if (!(value >= 1.0) || value > 2147483648.0 || value != std::floor(value))
+            return fail(ctx, XK_ERR_INVALID, "wait_limit must be an integer in 1..2^31");
+        ctx->prws.ctl.wait_limit = (uint32_t)value;
+        ctx->fresnel.wait_limit = (uint32_t)value;
+    } else if (n == "inject_stall") {
+        if (!(value >= 0.0) || value > 1024.0 || std::fmod(value, 16.0) != 0.0)
+            return fail(ctx, XK_ERR_INVALID, "inject_stall must be a multiple of 16 in 0..1024");
+        ctx->prws.ctl.stall_bytes = (uint32_t)value;
     } else {
         return fail(ctx, XK_ERR_INVALID, "unknown option");
     }

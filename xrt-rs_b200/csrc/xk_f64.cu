@@ -294,11 +294,51 @@ static_assert(kNoAllocScratchBytes == XK_NOALLOC_SCRATCH_BYTES, "header and scra
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch per device, looked up once with that
-// device current (a host-side reference to the symbol is not a device address).
+// Device address of g_noalloc_scratch per device, looked up with that device
+// current (a host-side reference to the symbol is not a device address). The
+// address belongs to the context the module was loaded into: the cache keeps
+// that context's unique id and looks the address up again when the current
+// context differs (after cudaDeviceReset the module is loaded anew, possibly
+// elsewhere).
 constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocSlot {
+    unsigned long long ctx_id = 0;  // 0: not looked up yet
+    void* addr = nullptr;
+};
 std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices];
+
+// cuCtxGetCurrent / cuCtxGetId, resolved through the runtime (the library does
+// not link the driver library itself).
+using CtxGetCurrentFn = int (*)(void** ctx);
+using CtxGetIdFn = int (*)(void* ctx, unsigned long long* id);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+bool g_ctx_fns_resolved = false;
+
+// Unique id of the calling thread's current context, 0 if there is none or it
+// cannot be told. Called with g_noalloc_mu held.
+unsigned long long current_ctx_id() {
+    if (!g_ctx_fns_resolved) {
+        g_ctx_fns_resolved = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f);
+        cudaGetLastError();
+    }
+    if (!g_ctx_get_current || !g_ctx_get_id) return 0;
+    void* c = nullptr;
+    if (g_ctx_get_current(&c) != 0 || !c) return 0;
+    unsigned long long id = 0;
+    if (g_ctx_get_id(c, &id) != 0) return 0;
+    return id;
+}
 
 }  // namespace
 }  // namespace xk
@@ -325,15 +365,20 @@ extern "C" int xk_diffraction_f64_noalloc(const xk_rays* rays, size_t n_rays,
     void* base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
+        NoAllocSlot& slot = g_noalloc_slot[dev];
+        const unsigned long long id = current_ctx_id();
+        if (slot.ctx_id == 0 || id != slot.ctx_id) {
+            // First call on this device, a thread whose context the driver
+            // does not report yet, or a context created since the lookup.
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
                 cudaGetLastError();
                 return XK_ERR_CUDA;
             }
-            g_noalloc_addr[dev] = p;
+            slot.addr = p;
+            slot.ctx_id = current_ctx_id();  // the lookup made the context current
         }
-        base = g_noalloc_addr[dev];
+        base = slot.addr;
     }
     int num_sms = 0;
     if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {

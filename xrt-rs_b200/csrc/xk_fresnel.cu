@@ -136,6 +136,7 @@ struct FusedArgs {
     double* partial;   // [splits][m_pad][n_pad]
     int m_pad, n_pad;
     int* err;
+    uint32_t wait_limit;  // polls of every bounded mbarrier wait
 };
 
 // Byte offset of 16-byte chunk c (0..7) of row r in a 128-byte-swizzled tile.
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             bool good = true;
             for (int q = 0; q < nseg && good; ++q) {
                 const int b = q & 1, use = q >> 1;
-                if (use >= 1 && !mbar_wait(&acc_empty[b], (uint32_t)(use - 1) & 1u)) {
+                if (use >= 1 && !mbar_wait(&acc_empty[b], (uint32_t)(use - 1) & 1u, g.wait_limit)) {
                     *flag = 1;
                     break;
                 }
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
                 const int i0 = q * kFSeg, i1 = min(nrb, i0 + kFSeg);
                 for (int i = i0; i < i1; ++i) {
                     const int s = i % kFStages;
-                    if (!mbar_wait(&full[s], (uint32_t)(i / kFStages) & 1u)) {
+                    if (!mbar_wait(&full[s], (uint32_t)(i / kFStages) & 1u, g.wait_limit)) {
                         *flag = 1;
                         good = false;
                         break;
@@ -293,7 +294,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
                 for (int c = 0; c < kFN; c += 32) rows0[(size_t)rr * g.n_pad + c] = 0.0;
         for (int q = 0; q < nseg; ++q) {
             const int b = q & 1;
-            const bool ok = mbar_wait(&acc_full[b], (uint32_t)(q >> 1) & 1u);
+            const bool ok = mbar_wait(&acc_full[b], (uint32_t)(q >> 1) & 1u, g.wait_limit);
             if (!__all_sync(0xffffffffu, ok)) {
                 *flag = 1;
                 break;
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             const int s = i % kFStages, rbuf = i & 1;
             RawRay nxt{g.ox, g.oz, 0.0, 0.0};
             if (i + 1 < nrb) fetch(i + 1, &nxt);  // in flight during this block
-            if (!mbar_wait(&empty[s], ((uint32_t)(i / kFStages) & 1u) ^ 1u)) *flag = 1;
+            if (!mbar_wait(&empty[s], ((uint32_t)(i / kFStages) & 1u) ^ 1u, g.wait_limit)) *flag = 1;
             unsigned char* base = tiles + (size_t)s * kFStage;
             const float4* sr = stage(rbuf);
 #pragma unroll 1
@@ -602,6 +603,7 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     fa.m_pad = (int)sh.m_pad;
     fa.n_pad = (int)sh.n_pad;
     fa.err = d_err;
+    fa.wait_limit = ws.wait_limit;
     const dim3 grid((unsigned)(sh.m_pad / 128), (unsigned)(sh.n_pad / kFN), (unsigned)sh.splits);
     const bool timed = rep->ev_gemm[0] && rep->ev_gemm[1];
     if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[0], stream));

@@ -845,11 +845,13 @@ struct WarpPipe {
     uint32_t phase;  // bit b: parity of the next completion of buffer b
 };
 
+// `extra` bytes beyond the copy are expected only by the stall test hook
+// (PrCtl::stall_bytes); 0 otherwise.
 __device__ __forceinline__ void issue_stage(WarpPipe& wp, int b, const PrRawRay* src, int len,
-                                            int lane) {
+                                            int lane, uint32_t extra = 0) {
     if (lane == 0) {
         uint32_t bytes = (uint32_t)len * (uint32_t)sizeof(PrRawRay);
-        mbar_arrive_expect_tx(wp.bar[b], bytes);
+        mbar_arrive_expect_tx(wp.bar[b], bytes + extra);
         bulk_g2s(wp.buf[b], src, bytes, wp.bar[b]);
     }
 }
@@ -867,7 +869,7 @@ __device__ __forceinline__ int chunk_of(const int* __restrict__ begin, int n_chu
 // Processes one (tile, ray-range) item; false if a bounded wait ran out.
 template <bool UNIFORM, bool FAST, bool FOLD, bool POL>
 __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, WarpShared& ws,
-                             int lane) {
+                             int lane, uint32_t wait_limit, uint32_t stall_bytes) {
     // local = (sub * groups + g) * n_tiles + t: sub-range `sub` of ray group g
     // against tile t. Sub-items of one (g, t) add into the same slots, so a
     // launch must never hold two of them (launches cover at most
@@ -897,7 +899,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
     int c = chunk_of(cb, n_chunks, pos);
     int len = min(kPrStage, min(cb[c + 1], r1) - pos);
     int b = 0;
-    issue_stage(wp, b, sv.recs + pos, len, lane);
+    issue_stage(wp, b, sv.recs + pos, len, lane, stall_bytes);
     while (true) {
         // Next stage: same chunk, or the next one at a chunk boundary.
         const int npos = pos + len;
@@ -908,12 +910,18 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
             nlen = min(kPrStage, min(cb[nc + 1], r1) - npos);
             issue_stage(wp, b ^ 1, sv.recs + npos, nlen, lane);
         }
-        const bool ok = mbar_wait(wp.bar[b], (wp.phase >> b) & 1u);
+        const uint32_t par = (wp.phase >> b) & 1u;
+        const bool ok = mbar_wait(wp.bar[b], par, wait_limit);
         wp.phase ^= (1u << b);
         if (!ok) {
-            // Wait (bounded) for the copy in flight on the other buffer.
+            // Before the warp leaves, give both buffers' copies another
+            // bounded wait, so that none is still writing into this warp's
+            // shared memory when the block exits: this stage's (a slow copy
+            // lands; a barrier that can never complete runs out again) and
+            // the next stage's, already issued.
+            mbar_wait(wp.bar[b], par, wait_limit);
             if (nlen > 0) {
-                mbar_wait(wp.bar[b ^ 1], (wp.phase >> (b ^ 1)) & 1u);
+                mbar_wait(wp.bar[b ^ 1], (wp.phase >> (b ^ 1)) & 1u, wait_limit);
                 wp.phase ^= (1u << (b ^ 1));
             }
             return false;
@@ -970,7 +978,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
 template <bool UNIFORM, bool FAST, bool FOLD, bool POL>
 __global__ void __launch_bounds__(kPrWarpsPerCta * 32, 3)
 pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long n_items,
-                     unsigned long long* __restrict__ counter, int* __restrict__ err) {
+                     unsigned long long* __restrict__ counter, int* __restrict__ err, PrCtl ctl) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     PrRawRay* bufs = reinterpret_cast<PrRawRay*>(smem) + warp * 2 * kPrStage;
@@ -1002,7 +1010,8 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
         }
         const PrSolve& sv = solves[lo];
         const long long local = item - sv.item_begin + sv.item_offset;
-        const bool ok = process_item<UNIFORM, FAST, FOLD, POL>(sv, local, wp, *wsh, lane);
+        const bool ok = process_item<UNIFORM, FAST, FOLD, POL>(
+            sv, local, wp, *wsh, lane, ctl.wait_limit, item == 0 ? ctl.stall_bytes : 0u);
         if (!ok) {
             if (lane == 0) atomicExch(err, 1);
             break;
@@ -1013,7 +1022,7 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
 constexpr size_t kPrSmemBytes = (size_t)kPrWarpsPerCta * 2 * kPrStage * sizeof(PrRawRay) +
                                 (size_t)kPrWarpsPerCta * sizeof(WarpShared);
 
-using PrKernel = void (*)(const PrSolve*, int, long long, unsigned long long*, int*);
+using PrKernel = void (*)(const PrSolve*, int, long long, unsigned long long*, int*, PrCtl);
 
 // Kernel of a variant: bit 0 uniform normal, bit 1 packed sweep, bit 2 folded
 // base phase, bit 3 one polarization (PrPlan::variant()).
@@ -1600,7 +1609,7 @@ Status pr_zero_partials(const PrPlan& P, cudaStream_t stream) {
 
 Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int variant,
                  unsigned long long* d_counter, int* d_err, cudaStream_t stream, int num_sms,
-                 int max_ctas_per_sm) {
+                 int max_ctas_per_sm, const PrCtl& ctl) {
     if (n_items <= 0) return Status::Ok();
     PrKernel kern = pr_kernel(variant);
     XK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1613,7 +1622,7 @@ Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int va
     long long grid = (long long)num_sms * per_sm;
     grid = std::max<long long>(1, std::min(grid, (n_items + kPrWarpsPerCta - 1) / kPrWarpsPerCta));
     kern<<<(unsigned)grid, kPrWarpsPerCta * 32, kPrSmemBytes, stream>>>(d_table, n_solves, n_items,
-                                                                        d_counter, d_err);
+                                                                        d_counter, d_err, ctl);
     XK_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
 }
@@ -1683,9 +1692,12 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
                                 cudaMemcpyHostToDevice, stream));
     if (time_kernels) XK_CUDA_TRY(cudaEventRecord(ws.ev[0], stream));
     int li = 0;
+    PrCtl ctl = ws.ctl;
+    ws.ctl.stall_bytes = 0;  // the stall test hook arms one execution only
     for (const Launch& L : launches) {
         XK_TRY(pr_launch(reinterpret_cast<const PrSolve*>(ws.solves.ptr) + L.first, L.count,
-                         L.items, L.variant, d_counters + li, d_err, stream, num_sms, 0));
+                         L.items, L.variant, d_counters + li, d_err, stream, num_sms, 0, ctl));
+        ctl.stall_bytes = 0;
         R.kernels += 1;
         R.n_items += L.items;
         ++li;

@@ -22,6 +22,16 @@ struct PrOptions {
     int polarization = -1;        // -1 automatic, 0 always sum Es and Ep separately
 };
 
+// Launch controls of the persistent kernel: the poll limit of every bounded
+// wait, and a test hook that arms the first ray stage of item 0 with
+// `stall_bytes` more than its bulk copy delivers, so that stage's barrier
+// never completes and the wait runs out (the copy itself lands; nothing is
+// left in flight). 0 in production.
+struct PrCtl {
+    uint32_t wait_limit = 1u << 24;
+    uint32_t stall_bytes = 0;
+};
+
 // Reasons a solve is routed to the FP64 path (xk_route_reason).
 constexpr int kRouteReasonCount = 9;
 extern const char* const kRouteReasons[kRouteReasonCount];
@@ -111,6 +121,7 @@ struct PrWorkspace {
     size_t host_bytes = 0;
     int* host_err = nullptr;  // error word copied back by the last execution
     bool host_borrowed = false;  // `host` belongs to the caller: never freed here
+    PrCtl ctl;                   // wait limit; stall_bytes is cleared after one execution
     Status ensure_host(size_t bytes);
     void release();
     // Stream-ordered allocation for every device buffer of this workspace.
@@ -151,7 +162,7 @@ Status pr_zero_partials(const PrPlan& P, cudaStream_t stream);
 constexpr int kPrVariants = 16;
 Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int variant,
                  unsigned long long* d_counter, int* d_err, cudaStream_t stream, int num_sms,
-                 int max_ctas_per_sm);
+                 int max_ctas_per_sm, const PrCtl& ctl = PrCtl{});
 Status pr_finalize(const PrPlan& P, cudaStream_t stream);
 
 // After the stream is synchronised: error flag and chunk counts.

@@ -65,9 +65,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Waits for the completion of the barrier phase of the given parity; false
-// if the iteration limit ran out first.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t it = 0; it < kMaxWaitIters; ++it)
+// if `limit` polls ran out first (each poll may itself suspend the thread for
+// a short, hardware-chosen time).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint32_t limit = kMaxWaitIters) {
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
