@@ -10,17 +10,16 @@ This script copies the numeric content (inputs and expected outputs, nothing
 else) into tests/golden/ so the suite does not need the reference checkout at
 run time.
 
-    python tests/golden/make_golden.py [path/to/diffraction_ref.json]
+    python tests/golden/make_golden.py path/to/xrt-rs/validation/fixtures/diffraction_ref.json
 """
 import json
 import os
 import sys
 
-DEFAULT_SRC = "/root/reference/validation/fixtures/diffraction_ref.json"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "diffraction_ref.json")
 
 
-def main(src: str = DEFAULT_SRC) -> None:
+def main(src: str) -> None:
     with open(src) as f:
         fix = json.load(f)
     cases = []
@@ -43,4 +42,6 @@ def main(src: str = DEFAULT_SRC) -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py path/to/validation/fixtures/diffraction_ref.json")
+    main(sys.argv[1])

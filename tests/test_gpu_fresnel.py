@@ -152,3 +152,26 @@ def test_separable_routes_to_f64_beyond_the_cross_term_bound(ctx, oracle):
     res, st = xrt_rs.fresnel_propagate(x, z, es, 30000.0, 100.0, sc, ctx=ctx, return_stats=True)
     assert st["path"] == xrt_rs._lib.XK_PATH_F64
     assert rel(res.amplitude, oracle_field(oracle, x, z, es, 30000.0, 100.0, sc)) < F64_TOL
+
+
+@pytest.mark.parametrize("geom", range(4))
+@pytest.mark.parametrize("kind", ["one", "two", "row16", "row97"])
+def test_closed_form_fields(ctx, geom, kind):
+    """Both device paths against closed-form fields (point sources, a Talbot
+    row summed as a geometric series): FP64 to 1e-10 (widened by the FP64
+    rounding of the largest phase), the tensor-core product to 1e-4."""
+    import fresnel_closed as F
+    import test_fresnel_closed_form as T
+
+    energy, dist, sc_t = T.GEOMS[geom]
+    x, z, e, exact = T.sources(kind, energy, dist)
+    sc = FresnelScreen(*sc_t)
+    xp, zp = F.screen_coords(*sc_t)
+    ref = exact(xp, zp)
+    res = xrt_rs.fresnel_propagate(x, z, e, energy, dist, sc, path="f64", ctx=ctx)
+    assert F.rel_l2(res.amplitude, ref) <= T.tol(F64_TOL, energy, dist, x, z, sc_t)
+    res, st = xrt_rs.fresnel_propagate(x, z, e, energy, dist, sc, path="separable", ctx=ctx,
+                                       return_stats=True)
+    err = F.rel_l2(res.amplitude, ref)
+    print(f"closed form {kind} E={energy} d={dist}: separable {err:.2e} path={st['path']}")
+    assert err <= SEP_TOL
