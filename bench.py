@@ -48,8 +48,6 @@ SFU_OPS_PER_PAIR = 4
 # 512^2 workload from an ncu capture of the full-size launch, by the number of
 # amplitude columns summed (two-column kernel: key False).
 DRAM_BYTES_CONFIG1 = {False: 513.6e6, True: 267.8e6}
-FMA_LANES_PER_SM = 128
-SFU_LANES_PER_SM = 16
 
 
 def parse():
@@ -65,7 +63,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--sweep", type=int, default=-1, help="-1 auto, 0 SFU reciprocal, 1 packed")
-    ap.add_argument("--phase-budget", type=float, default=512.0)
+    ap.add_argument("--phase-budget", type=float, default=512.0,
+                    help="cap on the FP32 residual phase [rad]")
+    ap.add_argument("--tolerance", type=float, default=1e-4,
+                    help="requested relative L2 error of the FP32 phase-reduced field; the "
+                         "planner derives the residual-phase budget from it")
     ap.add_argument("--polarization", type=int, default=-1, choices=[-1, 0],
                     help="-1: one amplitude column when all rays share a polarization; "
                          "0: always sum Es and Ep separately")
@@ -87,6 +89,12 @@ def parse():
                     help="serve: pairs per work item (0 = the server's default)")
     ap.add_argument("--reserve-sms", type=int, default=0,
                     help="serve: SMs left to planning (0 = the server's default)")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="single workload: skip the served-latency block")
+    ap.add_argument("--serve-window", type=float, default=30.0,
+                    help="single workload: arrival window of each served-latency stream [s]")
+    ap.add_argument("--serve-rate", type=float, default=25.0,
+                    help="single workload: the sustainable stream's arrival rate [1/s]")
     return ap.parse_args()
 
 
@@ -252,6 +260,7 @@ def run_batch(args):
     ctx = xrt_rs.GpuContext.new(0)
     ctx.set_option("sweep", args.sweep)
     ctx.set_option("phase_budget", args.phase_budget)
+    ctx.set_option("tolerance", args.tolerance)
     ctx.set_option("polarization", args.polarization)
     solves = synth.config3(seed=0, count=args.batch_count)
     pairs = float(sum(len(r["x"]) * len(p["x"]) for r, p, _ in solves))
@@ -333,6 +342,7 @@ def run_sweep(args):
     ctx = xrt_rs.GpuContext.new(0)
     ctx.set_option("sweep", args.sweep)
     ctx.set_option("phase_budget", args.phase_budget)
+    ctx.set_option("tolerance", args.tolerance)
     ctx.set_option("polarization", args.polarization)
     cells = []
     for e in synth.CONFIG2_ENERGIES:
@@ -447,7 +457,7 @@ def run_fresnel(args):
     achieved = algo_flops / (gemm / 1e3) / 1e12
     # DRAM bytes (read + write) of one fresnel_fused_kernel launch on the
     # 2^20-ray 512x512 workload, from a single-pass ncu capture of full-size
-    # launches (profiles/fresnel_fused_2p16x256sq_ncu.md); other sizes null.
+    # launches; other sizes report null.
     fr_traffic = 33.8e6 if (args.rays == 1 << 20 and args.grid == 512) else None
     cpu = None
     if not args.no_cpu:
@@ -480,7 +490,13 @@ def run_fresnel(args):
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": fr_traffic, "kernel_ms": gemm,
                      "peak_source": peak_source,
-                     "algorithmic_flops": algo_flops},
+                     "algorithmic_flops": algo_flops,
+                     # The sum itself is one complex multiply-add (8 flops) per
+                     # pair; the three f16 partial products that carry its
+                     # precision are counted above.
+                     "single_product_equivalent": {
+                         "flops": 8.0 * pairs, "achieved": achieved / 3.0,
+                         "frac": achieved / 3.0 / peak}},
         "cpu_baseline": cpu, "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -488,27 +504,28 @@ def run_fresnel(args):
     return 0
 
 
-def run_serve(args):
-    """Poisson request stream through the continuous-batching server.
+def serve_session(ctx, rate_hz: float, duration_s: float, drain_s: float, seed: int = 0,
+                  epoch_pairs: float = 0.0, item_pairs: float = 0.0, reserve_sms: int = 0):
+    """One Poisson request stream through the continuous-batching server.
 
     Request sizes follow the serving configuration (rays log-uniform in
     [1e4, 2e6], screen points log-uniform in [256, 1e6], E ~ U(1, 30) keV,
     d ~ U(100, 20000) mm, 30 % reuse a resident ray set). Rays are slices of a
     shared 2e6-ray Gaussian aperture with the request's energy, so requests
-    can be produced at the arrival rate; screens are square grids."""
+    can be produced at the arrival rate; screens are square grids. Requests
+    still unfinished `drain_s` after the arrival window are cancelled by the
+    shutdown and counted as unfinished; latencies are those of completed
+    requests."""
     import threading
 
-    import torch
     import xrt_rs
     from xrt_rs import synth
     from xrt_rs.serve import Server
 
-    torch.cuda.set_device(0)
-    ctx = xrt_rs.GpuContext.new(0)
-    reqs = synth.config4_requests(seed=0, rate_hz=args.rate, duration_s=args.duration)
+    reqs = synth.config4_requests(seed=seed, rate_hz=rate_hz, duration_s=duration_s)
     base = synth.gaussian_aperture(2_000_000, 0.1, 10_000.0, 30_000.0, seed=1)
-    srv = Server(ctx, hbm_budget_bytes=120e9, epoch_pairs=args.epoch_pairs,
-                 item_pairs=args.item_pairs, reserve_sms=args.reserve_sms)
+    srv = Server(ctx, hbm_budget_bytes=120e9, epoch_pairs=epoch_pairs,
+                 item_pairs=item_pairs, reserve_sms=reserve_sms)
     sets = {}
     lat, done_pairs, failures = [], [0.0], [0]
     lock = threading.Lock()
@@ -551,7 +568,7 @@ def run_serve(args):
                     failures[0] += 1
 
     stop = threading.Event()
-    deadline = time.perf_counter() + args.duration + args.drain + 5
+    deadline = time.perf_counter() + duration_s + drain_s
     waiters = [threading.Thread(target=waiter, daemon=True) for _ in range(8)]
     for w in waiters:
         w.start()
@@ -585,27 +602,38 @@ def run_serve(args):
     launched_in_window = srv.stats()["pairs_launched"]
     stop.set()
     for w in waiters:
-        w.join(timeout=args.drain + 30)
+        w.join(timeout=drain_s + 30)
     elapsed = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    ctx.close()
     lat_a = np.array(lat) if lat else np.array([np.nan])
-    line = {
-        "workload": "serve", "metric": "served latency and throughput", "rate_hz": args.rate,
-        "window_s": window, "elapsed_s": elapsed, "submitted": submitted,
-        "completed": len(lat), "failed_or_unfinished": submitted - len(lat),
+    offered = sum(r["n_rays"] * max(16, int(round(np.sqrt(r["n_pix"])))) ** 2
+                  for r in reqs) / duration_s / 1e9
+    return {
+        "rate_hz": rate_hz, "window_s": window, "elapsed_s": elapsed, "submitted": submitted,
+        "completed": len(lat), "unfinished": submitted - len(lat),
         "p50_ms": float(np.percentile(lat_a, 50)), "p90_ms": float(np.percentile(lat_a, 90)),
         "p99_ms": float(np.percentile(lat_a, 99)),
         "gpair_s_served": done_pairs[0] / elapsed / 1e9,
         # Pairs of all work items launched during the arrival window (partly
         # served requests included): the device throughput under this load.
         "gpair_s_launched_in_window": launched_in_window / window / 1e9,
-        "offered_gpair_s": sum(r["n_rays"] * max(16, int(round(np.sqrt(r["n_pix"])))) ** 2
-                               for r in reqs) / args.duration / 1e9,
+        "offered_gpair_s": offered,
         "epochs": st["epochs"], "peak_bytes": st["peak_bytes"], "hbm_budget_bytes": 120e9,
-        "data": "synthetic: rays sliced from one 2e6-ray aperture, square-grid screens",
     }
+
+
+def run_serve(args):
+    import torch
+    import xrt_rs
+
+    torch.cuda.set_device(0)
+    ctx = xrt_rs.GpuContext.new(0)
+    res = serve_session(ctx, args.rate, args.duration, args.drain, epoch_pairs=args.epoch_pairs,
+                        item_pairs=args.item_pairs, reserve_sms=args.reserve_sms)
+    ctx.close()
+    line = {"workload": "serve", "metric": "served latency and throughput", **res,
+            "data": "synthetic: rays sliced from one 2e6-ray aperture, square-grid screens"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -642,6 +670,7 @@ def main():
         raise RuntimeError("no CUDA device")
     ctx.set_option("sweep", args.sweep)
     ctx.set_option("phase_budget", args.phase_budget)
+    ctx.set_option("tolerance", args.tolerance)
     ctx.set_option("polarization", args.polarization)
 
     rays, screen = synth.config1(seed=rank, n_rays=args.rays, grid=args.grid)
@@ -782,42 +811,76 @@ def main():
                 "rel_l2_field_f32pr_vs_f64": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
                 "rel_l2_intensity_f32pr_vs_f64": float(np.linalg.norm(ia - ib) / np.linalg.norm(ib))}
 
-    # Roofline of the pair kernel: FP32-FMA / SFU pair rate at the sampled clock.
+    # Roofline of the pair kernel. It is bound by the FP32 FMA pipe and the
+    # MUFU unit; both peak rates are measured on this GPU (xk_probe_pipes:
+    # lane operations and MUFU results per SM clock) and scaled by the SM
+    # clock sampled during the timed region.
     props = torch.cuda.get_device_properties(dev)
     sms = props.multi_processor_count
     clk_mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
-    # With one common polarization the algorithm has one complex multiply-add
-    # per pair instead of two (4 FMA-pipe ops fewer).
+    pipes = xrt_rs.probe_pipes(ctx)
+    fma_rate = pipes["fma_lane_ops_per_clk_sm"]
+    mufu_rate = pipes["mufu_ops_per_clk_sm"]
     one_col = bool(stats["one_polarization"])
-    fma_ops = FMA_OPS_PER_PAIR - (4 if one_col else 0)
-    pair_per_clk_sm = min(FMA_LANES_PER_SM / fma_ops, SFU_LANES_PER_SM / SFU_OPS_PER_PAIR)
-    peak = sms * pair_per_clk_sm * clk_mhz * 1e6 / 1e9
+    # The sweep as issued, per ray x screen pair: FMA-pipe lane cycles (an
+    # f32x2 instruction holds the pipe for two lanes' worth) and MUFU results.
+    if stats["sweep"] == 1:
+        cyc, mufu = (17 if one_col else 21), 2
+    else:
+        cyc, mufu = (16 if one_col else 20), 3
+    ceiling = sms * min(fma_rate / cyc, mufu_rate / mufu) * clk_mhz * 1e6 / 1e9
     kms = float(np.mean(kern_ms))
     achieved = pairs / (kms / 1e3) / 1e9
-    # DRAM bytes (read + write) of one pr_persistent_kernel launch on this
-    # workload, from an ncu capture of the full-size launch
-    # (profiles/pr_persistent_config1_dram.md); other sizes report null.
-    full_size = n == 1 << 20 and args.grid == 512 and args.phase_budget == 512.0
+    # The reference formula's operation count (kirchhoff.wgsl:79-128, per-ray
+    # terms amortised): 34 FMA-pipe and 4 SFU operations per pair, 4 FMA-pipe
+    # fewer with one amplitude column. The kernel's phase decomposition needs
+    # fewer, so the ratio against this count can exceed 1.
+    fma_ops = FMA_OPS_PER_PAIR - (4 if one_col else 0)
+    algo_peak = sms * min(fma_rate / fma_ops, mufu_rate / SFU_OPS_PER_PAIR) * clk_mhz * 1e6 / 1e9
+    # DRAM bytes of one launch of this workload are not computed from sizes:
+    # they come from a single-pass ncu capture of the full-size launch of the
+    # default configuration, and are reported for that configuration only.
+    full_size = n == 1 << 20 and args.grid == 512 and stats["phase_bound_rad"] <= 512.0 + 1e-9
     traffic = (DRAM_BYTES_CONFIG1[one_col] if full_size else None)
-    roofline = {"bound": "fp32_sfu", "achieved": achieved, "peak": peak, "unit": UNIT,
-                "frac": achieved / peak, "traffic": traffic,
+    roofline = {"bound": "fp32_fma_pipe+mufu", "achieved": achieved, "peak": ceiling,
+                "unit": UNIT, "frac": achieved / ceiling, "traffic": traffic,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+                                   "full-size launch, this workload only" if traffic else None),
                 "kernel": "pr_persistent_kernel", "kernel_ms": kms,
-                "peak_source": (f"{sms} SMs x min(128 FP32 lanes / {fma_ops} FMA-pipe ops, "
-                                f"16 SFU lanes / {SFU_OPS_PER_PAIR} SFU ops) per pair x "
-                                f"{clk_mhz:.0f} MHz median SM clock sampled in the timed region"),
-                "algorithmic_ops_per_pair": {"fma_pipe": fma_ops, "sfu": SFU_OPS_PER_PAIR}}
-    if stats["sweep"] == 1:
-        # The packed uniform-normal sweep as issued: FMA-pipe cycles per pair
-        # (an f32x2 instruction holds the pipe two cycles for two pairs) and
-        # MUFU operations per pair.
-        cyc = 17 if one_col else 21
-        ceil = sms * min(FMA_LANES_PER_SM / cyc, SFU_LANES_PER_SM / 2) * clk_mhz * 1e6 / 1e9
-        roofline["kernel_issue_ceiling"] = {"fma_pipe_cycles_per_pair": cyc, "mufu_per_pair": 2,
-                                            "value": ceil, "frac": achieved / ceil}
+                "peak_source": (f"measured pipe rates {fma_rate:.1f} FMA-pipe lane ops and "
+                                f"{mufu_rate:.2f} MUFU results per SM clock (xk_probe_pipes) "
+                                f"x {sms} SMs x {clk_mhz:.0f} MHz median SM clock in the timed "
+                                f"region, over {cyc} FMA-pipe lane cycles and {mufu} MUFU "
+                                f"results per pair as the sweep issues them"),
+                "kernel_ops_per_pair": {"fma_pipe_lane_cycles": cyc, "mufu": mufu},
+                "measured_pipes": pipes,
+                "algorithmic_count_equivalent": {
+                    "fma_pipe_ops_per_pair": fma_ops, "sfu_ops_per_pair": SFU_OPS_PER_PAIR,
+                    "peak": algo_peak, "ratio": achieved / algo_peak}}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(rays, screen, args.cpu_seconds)
+
+    # Served latency (after the timed region, one GPU): the serving mix as a
+    # Poisson stream at a rate one B200 sustains and at the configuration's
+    # 200 req/s (about 8x what one B200 computes), each for a bounded window.
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        sust = serve_session(ctx, args.serve_rate, args.serve_window, 10.0, seed=0)
+        over = serve_session(ctx, 200.0, args.serve_window, 10.0, seed=1)
+        serve = {
+            "mix": "rays log-uniform [1e4, 2e6], screen points log-uniform [256, 1e6], "
+                   "E ~ U(1, 30) keV, d ~ U(100, 20000) mm, 30 % resident ray sets, "
+                   "HBM budget 120 GB, FP32 phase-reduced",
+            "p99_ms": sust["p99_ms"], "sustainable": sust, "offered_200_req_s": over}
+        if fp64:
+            # The FP64 path serves at most its single-solve rate: the offered
+            # work over that rate is how far its queue would fall behind.
+            serve["fp64_plain"] = {
+                "capacity_gpair_s": fp64["value"],
+                "sustainable_stream_load": sust["offered_gpair_s"] / fp64["value"],
+                "offered_200_load": over["offered_gpair_s"] / fp64["value"]}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -831,7 +894,7 @@ def main():
                    "groups": stats["groups"], "sweep": ["sfu_rcp", "packed_f32x2"][stats["sweep"]],
                    "amplitude_columns": 1 if stats["one_polarization"] else 2},
         "e2e": e2e, "fp64_plain": fp64, "two_amplitude_columns": two_col,
-        "roofline": roofline, "cpu_baseline": cpu,
+        "roofline": roofline, "cpu_baseline": cpu, "serve": serve,
         "clocks": clk, "gpu_launches": launches,
     }
     if rank == 0:

@@ -184,6 +184,21 @@ int xk_autotune(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_pixels
                 size_t n_pix, xk_field* out, double budget_ms, int apply,
                 xk_tune_result* result);
 
+/* Peak rates of the two pipes the phase-reduced pair kernel is bound by (no
+ * counterpart in the reference; a measurement aid for rooflines). */
+typedef struct xk_pipe_peaks {
+    double fma_lane_ops_per_clk_sm; /* FP32 FMA-pipe lane operations per SM clock
+                                       (an f32x2 FMA counts two) */
+    double mufu_ops_per_clk_sm;     /* sin/cos results of the MUFU unit per SM clock */
+    double sm_clock_mhz;            /* SM clock seen during the probe */
+    double fma_ms, mufu_ms;         /* device time of each probe */
+    int num_sms;
+} xk_pipe_peaks;
+
+/* Measures both rates with every SM busy (clock64 cycle counts of resident
+ * blocks, so the rates do not depend on the clock). Takes ~0.1 s. */
+int xk_probe_pipes(xk_ctx* ctx, xk_pipe_peaks* out);
+
 /* ---- single solves --------------------------------------------------------- */
 
 /* waves::diffraction::diffraction_integral (src/waves/diffraction.rs:56-64)

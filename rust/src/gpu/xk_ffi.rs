@@ -107,6 +107,17 @@ pub struct xk_tune_result {
 }
 
 #[repr(C)]
+#[derive(Clone, Copy, Default, Debug)]
+pub struct xk_pipe_peaks {
+    pub fma_lane_ops_per_clk_sm: f64,
+    pub mufu_ops_per_clk_sm: f64,
+    pub sm_clock_mhz: f64,
+    pub fma_ms: f64,
+    pub mufu_ms: f64,
+    pub num_sms: c_int,
+}
+
+#[repr(C)]
 #[derive(Clone, Copy)]
 pub struct xk_wave_params {
     pub center: [f64; 3],
@@ -289,6 +300,8 @@ unsafe extern "C" {
     pub fn xk_autotune(ctx: *mut xk_ctx, rays: *const xk_rays, n_rays: usize,
                        pixels: *const xk_pixels, n_pix: usize, out: *mut xk_field,
                        budget_ms: f64, apply: c_int, result: *mut xk_tune_result) -> c_int;
+
+    pub fn xk_probe_pipes(ctx: *mut xk_ctx, out: *mut xk_pipe_peaks) -> c_int;
 
     // single solves
     pub fn xk_diffraction_integral(ctx: *mut xk_ctx, rays: *const xk_rays, n_rays: usize,

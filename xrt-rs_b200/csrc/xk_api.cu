@@ -315,6 +315,10 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
     if (n == "phase_budget") {
         if (!(value > 0.0) || value > 1e5) return fail(ctx, XK_ERR_INVALID, "phase_budget out of range");
         ctx->pr_opts.phase_budget = value;
+    } else if (n == "tolerance") {
+        if (!(value >= 1e-7) || value > 1e-2)
+            return fail(ctx, XK_ERR_INVALID, "tolerance must be in [1e-7, 1e-2]");
+        ctx->pr_opts.tolerance = value;
     } else if (n == "sweep") {
         if (value != -1.0 && value != 0.0 && value != 1.0)
             return fail(ctx, XK_ERR_INVALID, "sweep must be -1, 0 or 1");

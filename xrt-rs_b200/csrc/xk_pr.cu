@@ -13,8 +13,9 @@
 //                       its turn count in FP64, sin/cos of the reduced turn,
 //   * exp(-i k u.rho)   per ray and item, FP64 argument reduction folded
 //                       into the ray's amplitudes,
-//   * exp(i k Delta)    per pair, FP32: |k Delta| <= phase_budget by
-//                       construction of the chunk grid.
+//   * exp(i k Delta)    per pair, FP32: |k Delta| <= the residual-phase
+//                       budget by construction of the chunk grid (the budget
+//                       follows from the requested tolerance).
 // This generalises the reference's single-centroid reduction
 // (src/gpu/shaders/kirchhoff.wgsl:95-113, src/gpu/kirchhoff.rs:96-104,
 // 276-297), whose FP32 residual is unbounded at high Fresnel numbers.
@@ -1483,14 +1484,15 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             return std::sqrt(sq);
         };
         double cell[3];
+        const double budget = effective_phase_budget(opt);
         double h_hi = 2.0 * std::max(ext[0], std::max(ext[1], ext[2])) + 1e-300;
         double h_lo = 0.0;
-        if (phase_bound(k, a_max, cell_radius(h_hi, cell), I.d_lo) <= opt.phase_budget) {
+        if (phase_bound(k, a_max, cell_radius(h_hi, cell), I.d_lo) <= budget) {
             h_lo = h_hi;
         } else {
             for (int it = 0; it < 200; ++it) {
                 double h = 0.5 * (h_lo + h_hi);
-                if (phase_bound(k, a_max, cell_radius(h, cell), I.d_lo) <= opt.phase_budget) h_lo = h;
+                if (phase_bound(k, a_max, cell_radius(h, cell), I.d_lo) <= budget) h_lo = h;
                 else h_hi = h;
             }
         }

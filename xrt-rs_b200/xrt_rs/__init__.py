@@ -330,6 +330,16 @@ def autotune(rays, pixels, out, ctx=None, budget_ms=3000.0, apply=True):
     return res.to_dict()
 
 
+def probe_pipes(ctx=None):
+    """Peak rates of the FP32 FMA pipe (lane operations, an f32x2 FMA counting
+    two) and of the MUFU unit (sin/cos results), per SM clock, measured on
+    the device with every SM busy."""
+    ctx = _require_ctx(ctx)
+    res = _lib.XkPipePeaks()
+    _lib.check(_lib.load().xk_probe_pipes(ctx.handle, ctypes.byref(res)), ctx.handle)
+    return res.to_dict()
+
+
 def _as_records(a, dtype):
     a = np.ascontiguousarray(a)
     if a.dtype != dtype:

@@ -110,6 +110,16 @@ class XkTuneResult(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class XkPipePeaks(ctypes.Structure):
+    _fields_ = [("fma_lane_ops_per_clk_sm", ctypes.c_double),
+                ("mufu_ops_per_clk_sm", ctypes.c_double), ("sm_clock_mhz", ctypes.c_double),
+                ("fma_ms", ctypes.c_double), ("mufu_ms", ctypes.c_double),
+                ("num_sms", ctypes.c_int)]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 XK_BATCH_DEVICE = 1
 XK_BATCH_NO_GRAPH = 2
 
@@ -193,6 +203,7 @@ _SIGNATURES = {
     "xk_diffraction_f64_noalloc": (ctypes.c_int, [
         ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels), ctypes.c_size_t,
         ctypes.POINTER(XkField), ctypes.c_void_p]),
+    "xk_probe_pipes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(XkPipePeaks)]),
     "xk_autotune": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.POINTER(XkRays), ctypes.c_size_t, ctypes.POINTER(XkPixels),
         ctypes.c_size_t, ctypes.POINTER(XkField), ctypes.c_double, ctypes.c_int,
