@@ -16,8 +16,14 @@ z = 1000 mm (2.75e11 ray x screen pairs per step), FP32 phase-reduced form.
 `--impl reference` times the reference's CPU algorithm (the oracle port, the
 reference's Rust cannot be built here) on the same workload's sample.
 
-Multi-GPU (torchrun): every rank runs its own replica of the workload (weak
-scaling, no data-path collective); timing is the max over ranks.
+Multi-GPU (torchrun): by default the one solve's screen is split into
+contiguous blocks, one per rank, and the blocks are all-gathered over NCCL
+each step (strong scaling); `--shard replica` runs an independent copy of the
+workload per rank instead (weak scaling). Timing is the max over ranks.
+
+After the timed region the default run also reports served latency: the
+serving mix as a Poisson stream through the continuous-batching server at a
+rate one B200 sustains and at 200 req/s (`serve`).
 """
 from __future__ import annotations
 
@@ -89,6 +95,11 @@ def parse():
                     help="serve: pairs per work item (0 = the server's default)")
     ap.add_argument("--reserve-sms", type=int, default=0,
                     help="serve: SMs left to planning (0 = the server's default)")
+    ap.add_argument("--shard", choices=["screen", "replica"], default="screen",
+                    help="N > 1: 'screen' splits the one solve's screen across the ranks "
+                         "(strong scaling, blocks all-gathered on the GPUs each step); "
+                         "'replica' runs an independent copy of the workload per rank "
+                         "(weak scaling)")
     ap.add_argument("--no-serve", action="store_true",
                     help="single workload: skip the served-latency block")
     ap.add_argument("--serve-window", type=float, default=30.0,
@@ -673,16 +684,28 @@ def main():
     ctx.set_option("tolerance", args.tolerance)
     ctx.set_option("polarization", args.polarization)
 
-    rays, screen = synth.config1(seed=rank, n_rays=args.rays, grid=args.grid)
+    from xrt_rs import parallel
+
+    # Screen sharding: every rank holds the same rays and solves a contiguous
+    # block of the one screen; replicas: every rank its own seeded copy.
+    shard = args.shard == "screen"
+    rays, screen = synth.config1(seed=0 if shard else rank, n_rays=args.rays, grid=args.grid)
     fields = xrt_rs.RAY_FIELDS
+    m_total = len(screen["x"])
+    blk0, blk1 = parallel.shard_range(m_total, rank, world) if shard else (0, m_total)
     d_rays = [torch.from_numpy(rays[k]).to(dev) for k in fields]
-    d_pix = [torch.from_numpy(screen[k]).to(dev) for k in "xyz"]
-    m = len(screen["x"])
+    d_pix_full = [torch.from_numpy(screen[k]).to(dev) for k in "xyz"]
+    d_pix = [t[blk0:blk1] for t in d_pix_full]  # contiguous views of this rank's block
+    m = blk1 - blk0
     n = len(rays["x"])
     d_out = [torch.zeros(m, dtype=torch.float64, device=dev) for _ in range(4)]
+    gather = shard and world > 1
+    d_full = ([torch.zeros(m_total, dtype=torch.float64, device=dev) for _ in range(4)]
+              if gather else None)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
-    pairs = float(n) * float(m)
+    pairs = float(n) * float(m)  # this rank's
+    pairs_job = float(n) * float(m_total) if shard else pairs * world
 
     def barrier():
         if world > 1:
@@ -693,8 +716,14 @@ def main():
         return xrt_rs.diffraction_integral_device(d_rays, d_pix, d_out, path=path, ctx=ctx,
                                                   stream=stream.cuda_stream)
 
+    def step():
+        st = solve("f32pr")
+        if gather:  # the field's blocks, GPU to GPU over NCCL
+            parallel.gather_field_device(d_out, m_total, out=d_full)
+        return st
+
     for _ in range(args.warmup):
-        solve("f32pr")
+        step()
     torch.cuda.synchronize()
 
     clocks = ClockSampler(dev.index)
@@ -708,7 +737,7 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        stats = solve("f32pr")
+        stats = step()
         e1.record(stream)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
@@ -719,9 +748,8 @@ def main():
     clk = clocks.stop()
     ms = float(np.mean(step_ms))
     if world > 1:
-        from xrt_rs import parallel
         ms = parallel.max_over_ranks(ms)
-    value = pairs * world / (ms / 1e3) / 1e9
+    value = pairs_job / (ms / 1e3) / 1e9
     out32 = [t.cpu().numpy() for t in d_out]
 
     # The same solve with Es and Ep summed separately (what any input without
@@ -746,34 +774,49 @@ def main():
         b = np.concatenate([o2[0] + 1j * o2[1], o2[2] + 1j * o2[3]])
         tms_mean = float(np.mean(tms))
         if world > 1:
-            from xrt_rs import parallel
             tms_mean = parallel.max_over_ranks(tms_mean)
-        two_col = {"value": pairs * world / (tms_mean / 1e3) / 1e9, "unit": UNIT,
+        two_col = {"value": pairs_job / (tms_mean / 1e3) / 1e9, "unit": UNIT,
                    "ms_per_step": tms_mean, "steps": 3,
                    "rel_l2_field_vs_one_column": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
 
     # End to end through the host C ABI: pinned host inputs -> field on host.
+    # With screen sharding on N > 1 ranks each rank solves its block from
+    # host memory and the field is all-gathered (xrt_rs.parallel.solve_sharded).
     e2e = None
     if not args.no_e2e:
-        h_rays = [torch.from_numpy(rays[k]).pin_memory().numpy() for k in fields]
-        h_pix = [torch.from_numpy(screen[k]).pin_memory().numpy() for k in "xyz"]
-        xrt_rs.diffraction_integral(h_rays, h_pix, path="f32pr", ctx=ctx)
+        h_rays = {k: torch.from_numpy(rays[k]).pin_memory().numpy() for k in fields}
+        h_pix = {k: torch.from_numpy(screen[k]).pin_memory().numpy() for k in "xyz"}
+        h_blk = {k: v[blk0:blk1] for k, v in h_pix.items()}
+
+        def e2e_step():
+            if gather:
+                parallel.solve_sharded(h_rays, h_pix, path="f32pr", ctx=ctx)
+                return None
+            return xrt_rs.diffraction_integral(h_rays, h_blk, path="f32pr", ctx=ctx,
+                                               return_stats=True)[1]
+
+        e2e_step()
         times = []
         st = None
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
+            barrier()
             t0 = time.perf_counter()
-            _, st = xrt_rs.diffraction_integral(h_rays, h_pix, path="f32pr", ctx=ctx,
-                                                return_stats=True)
+            st = e2e_step()
             times.append(time.perf_counter() - t0)
         e2e_ms = 1e3 * float(np.mean(times))
         if world > 1:
-            from xrt_rs import parallel
             e2e_ms = parallel.max_over_ranks(e2e_ms)
-        e2e = {"value": pairs * world / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
-               "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(st["h2d_bytes"]),
-               "d2h_bytes_per_step": int(st["d2h_bytes"])}
+        if st is not None:
+            h2d, d2h = int(st["h2d_bytes"]), int(st["d2h_bytes"])
+        else:  # rays + this rank's block up, its field down, and the gather
+            width = max(b - a for a, b in (parallel.shard_range(m_total, r, world)
+                                           for r in range(world)))
+            h2d = 96 * n + 24 * m + 32 * width
+            d2h = 32 * m + 32 * width * world
+        e2e = {"value": pairs_job / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
+               "ms_per_step": e2e_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     # The plain FP64 form on the same inputs, and the FP32 form's error vs it.
     fp64 = None
@@ -840,7 +883,7 @@ def main():
     # DRAM bytes of one launch of this workload are not computed from sizes:
     # they come from a single-pass ncu capture of the full-size launch of the
     # default configuration, and are reported for that configuration only.
-    full_size = n == 1 << 20 and args.grid == 512 and stats["phase_bound_rad"] <= 512.0 + 1e-9
+    full_size = n == 1 << 20 and m == 512 * 512 and stats["phase_bound_rad"] <= 512.0 + 1e-9
     traffic = (DRAM_BYTES_CONFIG1[one_col] if full_size else None)
     roofline = {"bound": "fp32_fma_pipe+mufu", "achieved": achieved, "peak": ceiling,
                 "unit": UNIT, "frac": achieved / ceiling, "traffic": traffic,
@@ -884,11 +927,13 @@ def main():
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if shard else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": single_workload(n, args.grid),
-                   "rays": n, "screen_points": m, "pairs_per_step": pairs,
-                   "parallelism": f"replica x{world}", "l2": "flushed between steps (256 MiB write)",
+                   "rays": n, "screen_points": m_total, "pairs_per_step": pairs_job,
+                   "parallelism": (f"screen-sharded x{world}" if shard else f"replica x{world}"),
+                   "l2": "flushed between steps (256 MiB write)",
                    "path": "f32pr", "phase_bound_rad": stats["phase_bound_rad"],
                    "n_tiles": stats["n_tiles"], "n_chunks": stats["n_chunks"],
                    "groups": stats["groups"], "sweep": ["sfu_rcp", "packed_f32x2"][stats["sweep"]],

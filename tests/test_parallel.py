@@ -76,3 +76,56 @@ def test_two_gloo_ranks_shard_and_gather(tmp_path, oracle):
         for c in range(4):
             assert np.array_equal(got[f"arr_{c}"], ref[c])
         assert float(got["worst"]) == 11.0
+
+
+def _rank_device_gather(rank, world, port, result_dir):
+    import datetime
+    import sys
+
+    import torch
+    import torch.distributed as dist
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root, os.path.join(root, "xrt-rs_b200"), os.path.join(root, "tests")]
+    from oracle import oracle as orc
+    from xrt_rs import parallel as par
+    from xrt_rs import synth as syn
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    rays, screen = syn.config0(seed=4)
+    rays = {k: v[:800] for k, v in rays.items()}
+    keys = ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re", "ep_im", "energy")
+    # The screen-sharded bench step: this rank's block of the screen as
+    # views of the full columns, its field into block tensors, one gather.
+    m = len(screen["x"])
+    a, b = par.shard_range(m, rank, world)
+    full_pix = [torch.from_numpy(screen[k]) for k in "xyz"]
+    block = [t[a:b] for t in full_pix]
+    local = orc.kahan_f64([rays[k] for k in keys], [t.numpy() for t in block], threads=1)
+    local_t = [torch.from_numpy(np.ascontiguousarray(c)) for c in local]
+    out = [torch.full((m,), float("nan"), dtype=torch.float64) for _ in range(4)]
+    par.gather_field_device(local_t, m, out=out)
+    np.savez(os.path.join(result_dir, f"dev{rank}.npz"), *[t.numpy() for t in out])
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_device_gather_of_screen_blocks(tmp_path, oracle, world):
+    """gather_field_device (the all-gather of the strong-scaling bench step)
+    with gloo ranks on CPU tensors: every rank ends with the full field, equal
+    bit for bit to the unsharded solve, for even and uneven blocks."""
+    import torch.multiprocessing as mp
+
+    mp.start_processes(_rank_device_gather, args=(world, _free_port(), str(tmp_path)),
+                       nprocs=world, join=True, start_method="spawn")
+    rays, screen = synth.config0(seed=4)
+    rays = {k: v[:800] for k, v in rays.items()}
+    ref = oracle.kahan_f64(*cases.as_lists(rays, screen))
+    for rank in range(world):
+        got = np.load(tmp_path / f"dev{rank}.npz")
+        for c in range(4):
+            assert np.array_equal(got[f"arr_{c}"], ref[c])

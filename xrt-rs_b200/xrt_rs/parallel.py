@@ -2,9 +2,12 @@
 
 Screen points are independent, so a solve shards by screen point with no
 exchange during the compute: every rank solves a contiguous block of the
-screen on its own GPU, and the blocks are gathered once at the end. The
-benchmark's multi-GPU mode runs independent replicas instead (weak scaling);
-both time a step as the maximum over ranks.
+screen on its own GPU, and the blocks are gathered once at the end. With
+device-resident blocks the gather is one all-gather of a (4, block) tensor
+per rank over NCCL (NVLink), and the field never leaves the GPUs. The
+benchmark's multi-GPU mode shards one solve this way (strong scaling) or runs
+independent replicas (weak scaling); both time a step as the maximum over
+ranks.
 """
 from __future__ import annotations
 
@@ -51,6 +54,37 @@ def gather_field(local, n_total: int, group=None):
         for c in range(4):
             out[c][ra:rb] = blk[c, : rb - ra]
     return tuple(out)
+
+
+def gather_field_device(local, n_total: int, out=None, group=None):
+    """All-gather this rank's block of the field, four 1-D tensors on its
+    device (lengths from shard_range), into four full tensors on every rank
+    (`out`, or new ones). One all-gather of a (4, width) tensor per rank: on
+    NCCL the blocks move GPU to GPU; the gloo backend (CPU tensors) serves
+    the host-side tests."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    sizes = [shard_range(n_total, r, world) for r in range(world)]
+    width = max(b - a for a, b in sizes)
+    dev = local[0].device
+    a, b = sizes[rank]
+    mine = torch.zeros(4, width, dtype=torch.float64, device=dev)
+    for c in range(4):
+        mine[c, : b - a].copy_(local[c])
+    gathered = torch.empty(world, 4, width, dtype=torch.float64, device=dev)
+    if dist.get_backend(group) == "nccl":
+        dist.all_gather_into_tensor(gathered, mine, group=group)
+    else:  # gloo has no single-tensor all-gather
+        dist.all_gather(list(gathered.unbind(0)), mine, group=group)
+    if out is None:
+        out = [torch.empty(n_total, dtype=torch.float64, device=dev) for _ in range(4)]
+    for r, (ra, rb) in enumerate(sizes):
+        for c in range(4):
+            out[c][ra:rb].copy_(gathered[r, c, : rb - ra])
+    return out
 
 
 def solve_sharded(rays, screen, compute=None, path="f32pr", ctx=None, group=None):
