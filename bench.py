@@ -68,7 +68,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--sweep", type=int, default=-1, help="-1 auto, 0 SFU reciprocal, 1 packed")
+    ap.add_argument("--sweep", type=int, default=-1,
+                    help="-1 auto, 0 SFU reciprocal, 1 packed (quadratic series), "
+                         "2 packed (linear series)")
     ap.add_argument("--phase-budget", type=float, default=512.0,
                     help="cap on the FP32 residual phase [rad]")
     ap.add_argument("--tolerance", type=float, default=1e-4,
@@ -869,6 +871,8 @@ def main():
     # f32x2 instruction holds the pipe for two lanes' worth) and MUFU results.
     if stats["sweep"] == 1:
         cyc, mufu = (17 if one_col else 21), 2
+    elif stats["sweep"] == 2:  # one f32x2 FMA fewer per pair of points
+        cyc, mufu = (16 if one_col else 20), 2
     else:
         cyc, mufu = (16 if one_col else 20), 3
     ceiling = sms * min(fma_rate / cyc, mufu_rate / mufu) * clk_mhz * 1e6 / 1e9
@@ -936,7 +940,7 @@ def main():
                    "l2": "flushed between steps (256 MiB write)",
                    "path": "f32pr", "phase_bound_rad": stats["phase_bound_rad"],
                    "n_tiles": stats["n_tiles"], "n_chunks": stats["n_chunks"],
-                   "groups": stats["groups"], "sweep": ["sfu_rcp", "packed_f32x2"][stats["sweep"]],
+                   "groups": stats["groups"], "sweep": ["sfu_rcp", "packed_f32x2", "packed_f32x2_linear_series"][stats["sweep"]],
                    "amplitude_columns": 1 if stats["one_polarization"] else 2},
         "e2e": e2e, "fp64_plain": fp64, "two_amplitude_columns": two_col,
         "roofline": roofline, "cpu_baseline": cpu, "serve": serve,

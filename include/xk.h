@@ -107,7 +107,8 @@ typedef struct xk_stats {
     double main_kernel_ms;   /* device time of the pair kernel alone (CUDA events) */
     int groups;              /* ray groups per tile (F32PR) */
     int routed_reason;       /* 0 = not routed; see xk_route_reason() */
-    int sweep;               /* F32PR sweep used: 0 SFU reciprocal, 1 packed + series, -1 none */
+    int sweep;               /* F32PR sweep used: 0 SFU reciprocal, 1 packed + quadratic series,
+                                2 packed + linear series, -1 none */
     int one_polarization;    /* F32PR: 1 if every ray had ray 0's polarization, so the kernel
                                 summed one amplitude column and Ep = (ep_0 / es_0) Es */
 } xk_stats;
@@ -143,8 +144,14 @@ const char* xk_route_reason(int reason);
 
 /* Tuning knobs of the F32PR path (no counterpart in the reference, whose
  * shader has no parameters). Names:
- *   "phase_budget"   bound on the FP32 residual phase in rad (default 512)
- *   "sweep"          -1 automatic, 0 SFU reciprocal, 1 packed f32x2 sweep
+ *   "phase_budget"   cap on the FP32 residual phase in rad (default 512)
+ *   "tolerance"      requested relative L2 error of the phase-reduced field
+ *                    (default 1e-4, range [1e-7, 1e-2]); the residual-phase
+ *                    budget is derived from it (and capped by "phase_budget")
+ *   "sweep"          -1 automatic, 0 SFU reciprocal, 1 packed f32x2 sweep with
+ *                    the quadratic series reciprocal, 2 packed with the linear
+ *                    series (automatic where its error stays below a tenth of
+ *                    the tolerance)
  *   "groups"         ray ranges per screen tile, 0 = automatic
  *   "items_per_warp" target work items per resident warp (automatic groups)
  *   "polarization"   -1 (default): when every ray's (es, ep) is a multiple of

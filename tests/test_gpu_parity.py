@@ -234,9 +234,10 @@ def sweep_ctx(ctx):
     ctx.set_option("sweep", -1)
 
 
-@pytest.mark.parametrize("sweep", [0, 1])
+@pytest.mark.parametrize("sweep", [0, 1, 2])
 def test_both_sweeps_config0(sweep_ctx, oracle, sweep):
-    """The SFU-reciprocal sweep and the packed f32x2 series sweep."""
+    """The SFU-reciprocal sweep and the packed f32x2 sweeps (quadratic and
+    linear series reciprocal)."""
     sweep_ctx.set_option("sweep", sweep)
     rays, pix = synth.config0(seed=3)
     ref = oracle_run(oracle, rays, pix)
@@ -246,7 +247,7 @@ def test_both_sweeps_config0(sweep_ctx, oracle, sweep):
     assert cases.rel_l2_intensity(out, ref) < PR_TOL
 
 
-@pytest.mark.parametrize("sweep", [0, 1])
+@pytest.mark.parametrize("sweep", [0, 1, 2])
 def test_both_sweeps_general_normals(sweep_ctx, oracle, sweep):
     sweep_ctx.set_option("sweep", sweep)
     rays, pix = cases.random_case(2000, 300, seed=21, general_normals=True)
@@ -315,3 +316,19 @@ def test_f64_reduction_option_keeps_parity(ctx, oracle):
             assert cases.rel_l2(out, oracle_run(oracle, r, p)) < F64_TOL
     finally:
         ctx.set_option("f64_reduction", 0)
+
+
+def test_linear_series_chosen_only_where_its_error_is_negligible(sweep_ctx, oracle):
+    """Automatic sweep: the linear series where |e|^2 x budget stays below a
+    tenth of the tolerance (e = u.rho / |q| <= b / (d - b), b the ray-chunk
+    radius), as on the 10 keV, 1 m workload; the quadratic one where chunks
+    are large for their distance (1 keV, 100 mm, a screen a few microns wide,
+    so e ~ 1e-3). Both within the tolerance of the extended-precision oracle."""
+    far, far_pix = synth.config1(seed=2, n_rays=1 << 14, grid=32)
+    near = synth.gaussian_aperture(1 << 14, 0.1, 1000.0, 30000.0, seed=3)
+    near_pix = synth.line_screen(64, 0.002, 100.0)
+    for rays, pix, want in ((far, far_pix, 2), (near, near_pix, 1)):
+        out, st = run(sweep_ctx, rays, pix, "f32pr")
+        assert st["sweep"] == want, st
+        rl, pl = cases.as_lists(rays, pix)
+        assert cases.rel_l2(out, oracle.kahan_ld(rl, pl)) < PR_TOL

@@ -123,7 +123,7 @@ xk::Status run_solve(xk_ctx* ctx, const xk::RaysDev& rays, size_t n_rays, const 
             stats->groups = P.groups;
             stats->routed_reason = P.routed ? P.route_reason : 0;
             stats->main_kernel_ms = er.main_kernel_ms;
-            stats->sweep = P.routed ? -1 : (P.fast ? 1 : 0);
+            stats->sweep = P.routed ? -1 : (P.fast ? (P.lin ? 2 : 1) : 0);
             stats->one_polarization = !P.routed && P.one_pol;
         }
     } else {
@@ -320,8 +320,8 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
             return fail(ctx, XK_ERR_INVALID, "tolerance must be in [1e-7, 1e-2]");
         ctx->pr_opts.tolerance = value;
     } else if (n == "sweep") {
-        if (value != -1.0 && value != 0.0 && value != 1.0)
-            return fail(ctx, XK_ERR_INVALID, "sweep must be -1, 0 or 1");
+        if (value != -1.0 && value != 0.0 && value != 1.0 && value != 2.0)
+            return fail(ctx, XK_ERR_INVALID, "sweep must be -1, 0, 1 or 2");
         ctx->pr_opts.sweep = (int)value;
     } else if (n == "groups") {
         if (value < 0.0 || value > 65536.0) return fail(ctx, XK_ERR_INVALID, "groups out of range");

@@ -745,8 +745,9 @@ __device__ __forceinline__ void clear_acc(PackedState<UNIFORM>& ls) {
         for (int c = 0; c < 4; ++c) ls.acc[i][c] = f2(0.f);
 }
 
-// SFU sweep: one point per FP32 instruction, rcp.approx for the reciprocal.
-template <bool UNIFORM, bool FOLD, bool POL>
+// SFU sweep: one point per FP32 instruction, rcp.approx for the reciprocal
+// (LIN does not apply).
+template <bool UNIFORM, bool FOLD, bool POL, bool LIN>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
                                             ScalarState<UNIFORM>& ls, WarpShared& ws) {
     const float4* rec = reinterpret_cast<const float4*>(buf);
@@ -785,8 +786,11 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
     }
 }
 
-// Packed sweep: two points per f32x2 instruction, series reciprocal.
-template <bool UNIFORM, bool FOLD, bool POL>
+// Packed sweep: two points per f32x2 instruction, series reciprocal
+// r0 (1 + e + e^2), or r0 (1 + e) when the planner bounds |e|^2 times the
+// phase budget far below the tolerance (LIN: one f32x2 FMA fewer per pair of
+// points).
+template <bool UNIFORM, bool FOLD, bool POL, bool LIN>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
                                             PackedState<UNIFORM>& ls, WarpShared& ws) {
     constexpr int H = kPrPpl / 2;
@@ -814,7 +818,8 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             num = __ffma2_rn(ls.vz[i], az, num);
             // 1/(2|q| - 2u.rho) = r0 / (1 - e), e = 2u.rho r0 ~ r0 (1 + e + e^2)
             const float2 ep = __fmul2_rn(wn, ls.q2[i]);
-            const float2 rd = __ffma2_rn(ls.q2[i], __ffma2_rn(ep, ep, ep), ls.q2[i]);
+            const float2 rd = LIN ? __ffma2_rn(ls.q2[i], ep, ls.q2[i])
+                                  : __ffma2_rn(ls.q2[i], __ffma2_rn(ep, ep, ep), ls.q2[i]);
             const float2 th = FOLD ? __ffma2_rn(num, rd, ls.phi[i]) : __fmul2_rn(num, rd);
             float s0, c0, s1, c1;
             __sincosf(th.x, &s0, &c0);
@@ -868,7 +873,7 @@ __device__ __forceinline__ int chunk_of(const int* __restrict__ begin, int n_chu
 }
 
 // Processes one (tile, ray-range) item; false if a bounded wait ran out.
-template <bool UNIFORM, bool FAST, bool FOLD, bool POL>
+template <bool UNIFORM, bool FAST, bool FOLD, bool POL, bool LIN>
 __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, WarpShared& ws,
                              int lane, uint32_t wait_limit, uint32_t stall_bytes) {
     // local = (sub * groups + g) * n_tiles + t: sub-range `sub` of ray group g
@@ -950,7 +955,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
         }
         prep_stage<POL>(wp.buf[b], len, lane, sv, ws);
         __syncwarp();
-        sweep_stage<UNIFORM, FOLD, POL>(wp.buf[b], len, lane, st, ws);
+        sweep_stage<UNIFORM, FOLD, POL, LIN>(wp.buf[b], len, lane, st, ws);
         // FP32 partials run over at most kFoldStages stages of one chunk.
         if (++since_fold == kFoldStages || nlen == 0 || nc != c) {
             fold_acc<POL>(st, ws, lane);
@@ -976,7 +981,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
 // sweep); solves[s].item_begin is the prefix sum of the item counts in this
 // launch, and the launch covers items [item_offset, item_offset + count) of
 // each solve.
-template <bool UNIFORM, bool FAST, bool FOLD, bool POL>
+template <bool UNIFORM, bool FAST, bool FOLD, bool POL, bool LIN>
 __global__ void __launch_bounds__(kPrWarpsPerCta * 32, 3)
 pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long n_items,
                      unsigned long long* __restrict__ counter, int* __restrict__ err, PrCtl ctl) {
@@ -1011,7 +1016,7 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
         }
         const PrSolve& sv = solves[lo];
         const long long local = item - sv.item_begin + sv.item_offset;
-        const bool ok = process_item<UNIFORM, FAST, FOLD, POL>(
+        const bool ok = process_item<UNIFORM, FAST, FOLD, POL, LIN>(
             sv, local, wp, *wsh, lane, ctl.wait_limit, item == 0 ? ctl.stall_bytes : 0u);
         if (!ok) {
             if (lane == 0) atomicExch(err, 1);
@@ -1026,14 +1031,25 @@ constexpr size_t kPrSmemBytes = (size_t)kPrWarpsPerCta * 2 * kPrStage * sizeof(P
 using PrKernel = void (*)(const PrSolve*, int, long long, unsigned long long*, int*, PrCtl);
 
 // Kernel of a variant: bit 0 uniform normal, bit 1 packed sweep, bit 2 folded
-// base phase, bit 3 one polarization (PrPlan::variant()).
+// base phase, bit 3 one polarization, bit 4 linear series (PrPlan::variant();
+// bit 4 only occurs with bit 1).
 template <bool POL>
 PrKernel pr_kernel_pol(int v) {
     static const PrKernel table[8] = {
-        pr_persistent_kernel<false, false, false, POL>, pr_persistent_kernel<true, false, false, POL>,
-        pr_persistent_kernel<false, true, false, POL>,  pr_persistent_kernel<true, true, false, POL>,
-        pr_persistent_kernel<false, false, true, POL>,  pr_persistent_kernel<true, false, true, POL>,
-        pr_persistent_kernel<false, true, true, POL>,   pr_persistent_kernel<true, true, true, POL>};
+        pr_persistent_kernel<false, false, false, POL, false>,
+        pr_persistent_kernel<true, false, false, POL, false>,
+        pr_persistent_kernel<false, true, false, POL, false>,
+        pr_persistent_kernel<true, true, false, POL, false>,
+        pr_persistent_kernel<false, false, true, POL, false>,
+        pr_persistent_kernel<true, false, true, POL, false>,
+        pr_persistent_kernel<false, true, true, POL, false>,
+        pr_persistent_kernel<true, true, true, POL, false>};
+    static const PrKernel lin[4] = {  // packed sweeps: uniform x folded
+        pr_persistent_kernel<false, true, false, POL, true>,
+        pr_persistent_kernel<true, true, false, POL, true>,
+        pr_persistent_kernel<false, true, true, POL, true>,
+        pr_persistent_kernel<true, true, true, POL, true>};
+    if ((v & 16) && (v & 2)) return lin[(v & 1) | ((v >> 1) & 2)];
     return table[v & 7];
 }
 
@@ -1530,7 +1546,13 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         // |e| = |u.rho| / |q| <= b / (d_lo - b): the series reciprocal's
         // argument.
         P.rcp_bound = b_max / std::max(I.d_lo - b_max, 1e-300);
-        P.fast = opt.sweep == 1 || (opt.sweep < 0 && P.rcp_bound <= kSeriesRcpBound);
+        P.fast = opt.sweep >= 1 || (opt.sweep < 0 && P.rcp_bound <= kSeriesRcpBound);
+        // The linear series drops r0 e^2: a relative error of at most e^2 in
+        // the reciprocal, |residual phase| e^2 in the phase (a bias shared by
+        // all pairs). Used where that stays below a tenth of the tolerance.
+        P.lin = P.fast && (opt.sweep == 2 ||
+                           (opt.sweep < 0 &&
+                            P.rcp_bound * P.rcp_bound * budget <= 0.1 * opt.tolerance));
         {
             // Fold the base phase into the sweep when ray groups span many
             // chunks (near field): per-chunk flushes then disappear, at the
@@ -1646,7 +1668,7 @@ Status pr_reserve_exec(PrWorkspace& ws, int count, int num_sms) {
     const HostLayout HL = host_layout(count, sum_blocks_for(num_sms));
     XK_TRY(ws.ensure_host(HL.total));
     XK_TRY(ws.solves.ensure(std::max<size_t>(1, count) * sizeof(PrSolve)));
-    XK_TRY(ws.ctrl.ensure(256));
+    XK_TRY(ws.ctrl.ensure(kPrCtrlBytes));
     if (!ws.ev[0]) XK_CUDA_TRY(cudaEventCreate(&ws.ev[0]));
     if (!ws.ev[1]) XK_CUDA_TRY(cudaEventCreate(&ws.ev[1]));
     return Status::Ok();
@@ -1665,8 +1687,8 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
     ws.host_err = reinterpret_cast<int*>(hbase + HL.err_off);
     *ws.host_err = 0;
     unsigned long long* d_counters = reinterpret_cast<unsigned long long*>(ws.ctrl.ptr);
-    int* d_err = reinterpret_cast<int*>(static_cast<char*>(ws.ctrl.ptr) + 128);
-    XK_CUDA_TRY(cudaMemsetAsync(ws.ctrl.ptr, 0, 256, stream));
+    int* d_err = reinterpret_cast<int*>(static_cast<char*>(ws.ctrl.ptr) + kPrCtrlErrOffset);
+    XK_CUDA_TRY(cudaMemsetAsync(ws.ctrl.ptr, 0, kPrCtrlBytes, stream));
 
     // Group the planned solves by kernel variant into contiguous tables.
     struct Launch {

@@ -20,7 +20,8 @@ struct PrOptions {
     // residual-phase budget from it (effective_phase_budget).
     double tolerance = 1e-4;
     int groups = 0;               // ray groups per tile; 0 = automatic
-    int sweep = -1;               // -1 automatic, 0 SFU reciprocal, 1 packed + Newton
+    int sweep = -1;               // -1 automatic, 0 SFU reciprocal, 1 packed + quadratic
+                                  // series reciprocal, 2 packed + linear series
     long long items_per_warp = 16;  // target items per resident warp (automatic groups)
     int polarization = -1;        // -1 automatic, 0 always sum Es and Ep separately
 };
@@ -105,15 +106,17 @@ struct PrPlan {
     bool uniform_normal = false;
     bool fast = false;  // packed sweep with Newton reciprocal
     bool fold = false;  // base phase folded into the per-pair phase (near field)
+    bool lin = false;   // packed sweep with the series reciprocal cut after the linear term
     // Every ray's (es, ep) is a multiple of one complex pair: the kernel sums
     // A = sum a_j U_j for one amplitude column and the field is
     // (Es, Ep) = (pol_es, pol_ep) * A.
     bool one_pol = false;
     double pol_es[2] = {1.0, 0.0}, pol_ep[2] = {0.0, 0.0};
     // Kernel variant: bit 0 uniform normal, bit 1 packed sweep, bit 2 folded,
-    // bit 3 one polarization.
+    // bit 3 one polarization, bit 4 linear series (packed sweep only).
     int variant() const {
-        return (uniform_normal ? 1 : 0) | (fast ? 2 : 0) | (fold ? 4 : 0) | (one_pol ? 8 : 0);
+        return (uniform_normal ? 1 : 0) | (fast ? 2 : 0) | (fold ? 4 : 0) | (one_pol ? 8 : 0) |
+               (fast && lin ? 16 : 0);
     }
     int n_tiles = 0, groups = 0, n_chunks = 0;
     double phase_bound = 0.0, rcp_bound = 0.0;
@@ -178,7 +181,11 @@ Status pr_execute_enqueue(std::vector<PrPlan>& plans, PrWorkspace& ws, cudaStrea
 // clear a plan's partial slots; one persistent launch over a device table of
 // solves (all of one variant) covering n_items items; a plan's final reduction.
 Status pr_zero_partials(const PrPlan& P, cudaStream_t stream);
-constexpr int kPrVariants = 16;
+constexpr int kPrVariants = 32;
+// Control block of a launch set: one item counter per variant, then the
+// error word.
+constexpr size_t kPrCtrlErrOffset = 8 * kPrVariants;
+constexpr size_t kPrCtrlBytes = kPrCtrlErrOffset + 64;
 Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int variant,
                  unsigned long long* d_counter, int* d_err, cudaStream_t stream, int num_sms,
                  int max_ctas_per_sm, const PrCtl& ctl = PrCtl{});

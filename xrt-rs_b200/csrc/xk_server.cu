@@ -375,9 +375,9 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
     }
     XK_CUDA_TRY(cudaMemcpyAsync(e.table.ptr, e.h_table, tab * sizeof(xk::PrSolve),
                                 cudaMemcpyHostToDevice, s->exec_stream));
-    XK_CUDA_TRY(cudaMemsetAsync(e.ctrl.ptr, 0, 256, s->exec_stream));
+    XK_CUDA_TRY(cudaMemsetAsync(e.ctrl.ptr, 0, xk::kPrCtrlBytes, s->exec_stream));
     unsigned long long* counters = e.ctrl.as<unsigned long long>();
-    int* d_err = reinterpret_cast<int*>(e.ctrl.as<char>() + 128);
+    int* d_err = reinterpret_cast<int*>(e.ctrl.as<char>() + xk::kPrCtrlErrOffset);
     const int sms = std::max(1, s->num_sms - std::max(0, s->opts.reserve_sms));
     XK_CUDA_TRY(cudaEventRecord(s->fork_ev, s->exec_stream));
     int forks = 0;
@@ -660,7 +660,7 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
     XK_CUDA_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
     for (EpochSlot& e : s->slots) {
         XK_TRY(e.table.ensure(kVariants * (size_t)std::max(1, s->opts.max_active) * sizeof(xk::PrSolve)));
-        XK_TRY(e.ctrl.ensure(256));
+        XK_TRY(e.ctrl.ensure(xk::kPrCtrlBytes));
         XK_CUDA_TRY(cudaMallocHost(&e.h_table,
                                    kVariants * (size_t)std::max(1, s->opts.max_active) * sizeof(xk::PrSolve)));
         XK_CUDA_TRY(cudaMallocHost(&e.h_err, 64));
