@@ -111,6 +111,7 @@ typedef struct xk_stats {
                                 2 packed + linear series, -1 none */
     int one_polarization;    /* F32PR: 1 if every ray had ray 0's polarization, so the kernel
                                 summed one amplitude column and Ep = (ep_0 / es_0) Es */
+    int tuned;               /* F32PR: 1 if the solve used autotuned settings of its bucket */
 } xk_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -184,9 +185,17 @@ typedef struct xk_tune_result {
 
 /* Autotuner (no counterpart in the reference): times the XK_PATH_F32PR solve
  * of this device-resident problem under candidate settings of the knobs above
- * (residual-phase budget, i.e. ray-chunk size, up to 512 rad; work items per
- * warp; sweep variant) until `budget_ms` of device time is spent, writes the
- * field into `out`, and with `apply` keeps the fastest settings on `ctx`. */
+ * (residual-phase budget, i.e. ray-chunk size, never above what the
+ * tolerance allows; work items per warp, i.e. ray groups per tile; sweep
+ * variant) until `budget_ms` of device time is spent, and writes the field
+ * into `out`. With `apply` the fastest settings are kept in the context's
+ * tuning cache for this problem's bucket — energy and ray/screen distance to
+ * the nearest power of two, ray and screen-point counts by their leading
+ * power of two — and every later F32PR solve of that bucket on the context
+ * (single calls, batches, servers created afterwards) uses them
+ * (xk_stats.tuned); the context's defaults do not change. Options
+ * "use_tuned" (1 default, 0 ignores the cache) and "clear_tuned" (any value)
+ * control the cache. */
 int xk_autotune(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_pixels* pixels,
                 size_t n_pix, xk_field* out, double budget_ms, int apply,
                 xk_tune_result* result);

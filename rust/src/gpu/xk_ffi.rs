@@ -93,6 +93,7 @@ pub struct xk_stats {
     pub routed_reason: c_int,
     pub sweep: c_int,
     pub one_polarization: c_int,
+    pub tuned: c_int,
 }
 
 #[repr(C)]

@@ -44,6 +44,7 @@ xk::Status create_ctx(int device, xk_ctx** out) {
     ctx->device = device;
     ctx->num_sms = prop.multiProcessorCount;
     ctx->name = prop.name;
+    ctx->pr_opts.tune = &ctx->tune;
     cudaError_t e1 = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     cudaError_t e2 = cudaEventCreate(&ctx->ev0);
     cudaError_t e3 = cudaEventCreate(&ctx->ev1);
@@ -115,7 +116,10 @@ xk::Status run_solve(xk_ctx* ctx, const xk::RaysDev& rays, size_t n_rays, const 
         XK_CUDA_TRY(cudaEventRecord(ctx->ev1, stream));
         XK_CUDA_TRY(cudaStreamSynchronize(stream));
         if (!P.routed) XK_TRY(xk::pr_execute_finish(plans, ctx->prws, &er));
+        ctx->last_energy_ev = P.energy_ev;
+        ctx->last_dist_mm = P.dist_mm;
         if (stats) {
+            stats->tuned = P.tuned ? 1 : 0;
             stats->n_tiles = P.n_tiles;
             stats->n_chunks = P.n_chunks;
             stats->n_items = (long long)P.n_tiles * P.groups;
@@ -336,6 +340,11 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
     } else if (n == "items_per_warp") {
         if (value < 1.0 || value > 4096.0) return fail(ctx, XK_ERR_INVALID, "items_per_warp out of range");
         ctx->pr_opts.items_per_warp = (long long)value;
+    } else if (n == "use_tuned") {
+        if (value != 0.0 && value != 1.0) return fail(ctx, XK_ERR_INVALID, "use_tuned is 0 or 1");
+        ctx->tune.use = value != 0.0;
+    } else if (n == "clear_tuned") {
+        ctx->tune.clear();
     } else if (n == "wait_limit") {
         if (!(value >= 1.0) || value > 2147483648.0 || value != std::floor(value))
             return fail(ctx, XK_ERR_INVALID, "wait_limit must be an integer in 1..2^31");
@@ -365,24 +374,26 @@ int xk_autotune(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_pixels
     const xk::FieldDev fd{out->es_re, out->es_im, out->ep_re, out->ep_im};
     const xk::PrOptions base = ctx->pr_opts;
     // Candidates: the defaults first, then larger and smaller residual-phase
-    // budgets (ray chunks grow with the budget; the FP32 error bound grows
-    // with it too, so the search stops at 512 rad), more or fewer items per
-    // warp, and the SFU sweep.
+    // budgets (ray chunks grow with the budget; the tolerance caps it, so no
+    // candidate loosens the error bound), more or fewer items per warp, and
+    // the sweeps. Trials ignore the tuning cache.
     struct Cand {
         double budget;
         long long ipw;
         int sweep;
     };
     const Cand cands[] = {{base.phase_budget, base.items_per_warp, base.sweep},
-                          {512.0, 32, -1}, {512.0, 8, -1}, {256.0, 16, -1}, {384.0, 16, -1},
-                          {512.0, 16, 0}, {256.0, 32, -1}, {256.0, 8, -1}, {128.0, 16, -1}};
+                          {512.0, 32, -1}, {512.0, 8, -1}, {192.0, 16, -1}, {384.0, 16, -1},
+                          {512.0, 16, 1},  {512.0, 16, 0}, {192.0, 32, -1}, {192.0, 8, -1},
+                          {128.0, 16, -1}, {512.0, 4, -1}, {96.0, 16, -1}};
     double spent = 0.0, best = 1e300;
     xk::PrOptions best_opt = base;
     int trials = 0;
     for (const Cand& c : cands) {
         if (trials > 0 && spent >= budget_ms) break;
         ctx->pr_opts = base;
-        ctx->pr_opts.phase_budget = std::min(c.budget, 512.0);
+        ctx->pr_opts.tune = nullptr;
+        ctx->pr_opts.phase_budget = std::min(c.budget, base.phase_budget);
         ctx->pr_opts.items_per_warp = c.ipw;
         ctx->pr_opts.sweep = c.sweep;
         xk_stats st;
@@ -403,7 +414,15 @@ int xk_autotune(xk_ctx* ctx, const xk_rays* rays, size_t n_rays, const xk_pixels
             best_opt = ctx->pr_opts;
         }
     }
-    ctx->pr_opts = apply ? best_opt : base;
+    ctx->pr_opts = base;
+    if (apply && trials > 0 && best < 1e299) {
+        // Kept for this problem's bucket; the context's own defaults stay.
+        xk::PrTuned t;
+        t.phase_budget = best_opt.phase_budget;
+        t.items_per_warp = best_opt.items_per_warp;
+        t.sweep = best_opt.sweep;
+        ctx->tune.store(ctx->last_energy_ev, ctx->last_dist_mm, n_rays, n_pix, t);
+    }
     result->best_ms = best < 1e299 ? best : result->default_ms;
     result->phase_budget = best_opt.phase_budget;
     result->items_per_warp = best_opt.items_per_warp;

@@ -1193,9 +1193,11 @@ int sum_blocks_for(int num_sms) { return std::min(512, std::max(1, 2 * num_sms))
 
 // Ray groups per tile: enough items to keep every resident warp busy, at
 // least four stages of rays per item, partial slots within 1 GiB.
-int plan_groups(int n, int n_tiles, int num_sms, const PrOptions& opt) {
+int plan_groups(int n, int m, int n_tiles, int num_sms, const PrOptions& opt) {
     if (opt.groups > 0) return std::min(opt.groups, kMaxGroups);
-    long long want = (long long)num_sms * 12 * opt.items_per_warp;
+    long long ipw = opt.items_per_warp;
+    if (opt.tune && opt.tune->use) opt.tune->find_ipw((size_t)n, (size_t)m, &ipw);
+    long long want = (long long)num_sms * 12 * ipw;
     int g = (int)std::max<long long>(1, (want + n_tiles - 1) / n_tiles);
     g = std::min(g, std::max(1, n / (4 * kPrStage)));
     long long cap = (1LL << 30) / (32LL * n_tiles * kPrTile);
@@ -1204,6 +1206,51 @@ int plan_groups(int n, int n_tiles, int num_sms, const PrOptions& opt) {
 }
 
 }  // namespace
+
+uint32_t PrTuneCache::size_key(size_t n, size_t m) {
+    const int nb = n ? std::ilogb((double)n) : 0, mb = m ? std::ilogb((double)m) : 0;
+    return (uint32_t)(nb & 0xff) << 8 | (uint32_t)(mb & 0xff);
+}
+
+uint64_t PrTuneCache::full_key(double energy_ev, double dist_mm, size_t n, size_t m) {
+    const int eb = energy_ev > 0 ? (int)std::lround(std::log2(energy_ev)) : 0;
+    const int db = dist_mm > 0 ? (int)std::lround(std::log2(dist_mm)) : 0;
+    return (uint64_t)((eb + 128) & 0xff) << 24 | (uint64_t)((db + 128) & 0xff) << 16 |
+           size_key(n, m);
+}
+
+void PrTuneCache::store(double energy_ev, double dist_mm, size_t n, size_t m, const PrTuned& t) {
+    std::lock_guard<std::mutex> lock(mu);
+    full[full_key(energy_ev, dist_mm, n, m)] = t;
+    ipw[size_key(n, m)] = t.items_per_warp;
+}
+
+bool PrTuneCache::find(double energy_ev, double dist_mm, size_t n, size_t m, PrTuned* t) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = full.find(full_key(energy_ev, dist_mm, n, m));
+    if (it == full.end()) return false;
+    *t = it->second;
+    return true;
+}
+
+bool PrTuneCache::find_ipw(size_t n, size_t m, long long* ipw_out) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = ipw.find(size_key(n, m));
+    if (it == ipw.end()) return false;
+    *ipw_out = it->second;
+    return true;
+}
+
+size_t PrTuneCache::size() {
+    std::lock_guard<std::mutex> lock(mu);
+    return full.size();
+}
+
+void PrTuneCache::clear() {
+    std::lock_guard<std::mutex> lock(mu);
+    full.clear();
+    ipw.clear();
+}
 
 const char* const kRouteReasons[kRouteReasonCount] = {
     "",
@@ -1247,7 +1294,7 @@ size_t pr_plan_bytes(size_t n, size_t m, int num_sms, const PrOptions& opt) {
     if (n == 0 || m == 0) return 0;
     const int sum_blocks = sum_blocks_for(num_sms);
     const int n_tiles = (int)((m + kPrTile - 1) / kPrTile);
-    const int g = plan_groups((int)n, n_tiles, num_sms, opt);
+    const int g = plan_groups((int)n, (int)m, n_tiles, num_sms, opt);
     Arena a{nullptr, 0};
     SolveBufs b;
     carve(a, b, (int)n, (int)m, n_tiles, g, sum_blocks);
@@ -1278,7 +1325,7 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             return Status::Err(XK_ERR_INVALID, "too many rays or screen points for one solve");
         const int n = (int)in[s].n, m = (int)in[s].m;
         n_tiles[s] = (m + kPrTile - 1) / kPrTile;
-        const int g = plan_groups(n, n_tiles[s], num_sms, opt);
+        const int g = plan_groups(n, m, n_tiles[s], num_sms, opt);
         groups[s] = g;
         size_t c1 = 0, c2 = 0, c3 = 0;
         XK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, c1, (uint64_t*)nullptr,
@@ -1410,6 +1457,10 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             I.pc[a] = f[17 + a] / (double)in[s].m;
         }
         I.d_lo = box_distance(I.rlo, I.rhi, I.plo, I.phi);
+        P.energy_ev = f[9];
+        P.dist_mm = std::sqrt((I.pc[0] - I.rc[0]) * (I.pc[0] - I.rc[0]) +
+                              (I.pc[1] - I.rc[1]) * (I.pc[1] - I.rc[1]) +
+                              (I.pc[2] - I.rc[2]) * (I.pc[2] - I.rc[2]));
         if (!(I.d_lo > 0)) {
             P.routed = true;
             P.route_reason = 4;
@@ -1478,6 +1529,16 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         const int n = (int)in[s].n;
         const double a_max = h_amax[s] * 1.001;
         const double k = I.k;
+        // Autotuned settings of this solve's bucket, if any.
+        PrOptions o = opt;
+        if (opt.tune && opt.tune->use) {
+            PrTuned t;
+            if (opt.tune->find(P.energy_ev, P.dist_mm, in[s].n, in[s].m, &t)) {
+                o.phase_budget = std::min(t.phase_budget, opt.phase_budget);
+                o.sweep = t.sweep;
+                P.tuned = true;
+            }
+        }
         CellGrid cg{};
         cg.fr = I.fr;
         cg.fr.ox = I.rc[0];
@@ -1500,7 +1561,7 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
             return std::sqrt(sq);
         };
         double cell[3];
-        const double budget = effective_phase_budget(opt);
+        const double budget = effective_phase_budget(o);
         double h_hi = 2.0 * std::max(ext[0], std::max(ext[1], ext[2])) + 1e-300;
         double h_lo = 0.0;
         if (phase_bound(k, a_max, cell_radius(h_hi, cell), I.d_lo) <= budget) {
@@ -1546,13 +1607,13 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
         // |e| = |u.rho| / |q| <= b / (d_lo - b): the series reciprocal's
         // argument.
         P.rcp_bound = b_max / std::max(I.d_lo - b_max, 1e-300);
-        P.fast = opt.sweep >= 1 || (opt.sweep < 0 && P.rcp_bound <= kSeriesRcpBound);
+        P.fast = o.sweep >= 1 || (o.sweep < 0 && P.rcp_bound <= kSeriesRcpBound);
         // The linear series drops r0 e^2: a relative error of at most e^2 in
         // the reciprocal, |residual phase| e^2 in the phase (a bias shared by
         // all pairs). Used where that stays below a tenth of the tolerance.
-        P.lin = P.fast && (opt.sweep == 2 ||
-                           (opt.sweep < 0 &&
-                            P.rcp_bound * P.rcp_bound * budget <= 0.1 * opt.tolerance));
+        P.lin = P.fast && (o.sweep == 2 ||
+                           (o.sweep < 0 &&
+                            P.rcp_bound * P.rcp_bound * budget <= 0.1 * o.tolerance));
         {
             // Fold the base phase into the sweep when ray groups span many
             // chunks (near field): per-chunk flushes then disappear, at the

@@ -1,6 +1,8 @@
 // FP32 phase-reduced Kirchhoff path: planner + persistent kernel.
 #pragma once
 
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "xk_internal.cuh"
@@ -13,6 +15,32 @@ constexpr int kPrStage = 64;          // rays per shared-memory stage
 constexpr int kPrPpl = 8;             // screen points per lane
 constexpr int kPrTile = 32 * kPrPpl;  // screen points per tile (one warp)
 
+// Settings the autotuner found best for one class of solves.
+struct PrTuned {
+    double phase_budget = 512.0;
+    long long items_per_warp = 16;
+    int sweep = -1;
+};
+
+// Autotuned settings per bucket of solves: (energy, distance, ray count,
+// screen-point count), each on a log2 scale (energy in eV and distance in mm
+// rounded to the nearest power of two, counts by their leading power of
+// two). The ray-group count is fixed before the planner knows energy and
+// distance, so items per warp is also kept per (ray count, screen count).
+struct PrTuneCache {
+    std::mutex mu;
+    std::map<uint64_t, PrTuned> full;
+    std::map<uint32_t, long long> ipw;
+    bool use = true;  // apply cached settings to matching solves
+    static uint32_t size_key(size_t n, size_t m);
+    static uint64_t full_key(double energy_ev, double dist_mm, size_t n, size_t m);
+    void store(double energy_ev, double dist_mm, size_t n, size_t m, const PrTuned& t);
+    bool find(double energy_ev, double dist_mm, size_t n, size_t m, PrTuned* t);
+    bool find_ipw(size_t n, size_t m, long long* ipw_out);
+    size_t size();
+    void clear();
+};
+
 // Planner knobs.
 struct PrOptions {
     double phase_budget = 512.0;  // cap on |FP32 residual phase| [rad]
@@ -24,6 +52,7 @@ struct PrOptions {
                                   // series reciprocal, 2 packed + linear series
     long long items_per_warp = 16;  // target items per resident warp (automatic groups)
     int polarization = -1;        // -1 automatic, 0 always sum Es and Ep separately
+    PrTuneCache* tune = nullptr;  // per-bucket settings that override the above, or null
 };
 
 // Launch controls of the persistent kernel: the poll limit of every bounded
@@ -120,6 +149,8 @@ struct PrPlan {
     }
     int n_tiles = 0, groups = 0, n_chunks = 0;
     double phase_bound = 0.0, rcp_bound = 0.0;
+    double energy_ev = 0.0, dist_mm = 0.0;  // the solve's energy and ray/screen box distance
+    bool tuned = false;                     // settings came from the tuning cache
     PrSolve dev{};
     const int* tile_perm = nullptr;  // slot -> original screen point, -1 = padding
     int m = 0;

@@ -70,6 +70,7 @@ class XkStats(ctypes.Structure):
         ("routed_reason", ctypes.c_int),
         ("sweep", ctypes.c_int),
         ("one_polarization", ctypes.c_int),
+        ("tuned", ctypes.c_int),
     ]
 
     def to_dict(self):
