@@ -371,6 +371,7 @@ typedef struct xk_solve_plan {
     int path, routed_reason, n_tiles, n_chunks, groups, sweep;
     double phase_bound_rad;
     int one_polarization;
+    int tuned;  /* 1 if the solve uses autotuned settings of its bucket */
 } xk_solve_plan;
 
 /* Copies host inputs to the device (unless XK_BATCH_DEVICE), plans every

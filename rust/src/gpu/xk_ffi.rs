@@ -222,6 +222,7 @@ pub struct xk_solve_plan {
     pub sweep: c_int,
     pub phase_bound_rad: f64,
     pub one_polarization: c_int,
+    pub tuned: c_int,
 }
 
 #[repr(C)]

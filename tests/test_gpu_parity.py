@@ -332,3 +332,49 @@ def test_linear_series_chosen_only_where_its_error_is_negligible(sweep_ctx, orac
         assert st["sweep"] == want, st
         rl, pl = cases.as_lists(rays, pix)
         assert cases.rel_l2(out, oracle.kahan_ld(rl, pl)) < PR_TOL
+
+
+def test_autotune_cache_per_bucket(oracle):
+    """xk_autotune with apply keeps its best settings for the problem's bucket
+    (energy, distance, ray count, screen count): later solves of that bucket,
+    single or batched, report `tuned` and stay within the tolerance of the
+    extended-precision oracle; a solve of another bucket, or with the cache
+    switched off, runs the defaults bit for bit as before."""
+    torch = pytest.importorskip("torch")
+    ctx = xrt_rs.GpuContext.new(0)
+    try:
+        rays, pix = synth.config0(seed=7)
+        rl, pl = cases.as_lists(rays, pix)
+        default, st0 = run(ctx, rays, pix, "f32pr")
+        assert st0["tuned"] == 0
+        d_r = [torch.from_numpy(a).cuda() for a in rl]
+        d_p = [torch.from_numpy(a).cuda() for a in pl]
+        d_o = [torch.zeros(len(pl[0]), dtype=torch.float64, device="cuda") for _ in range(4)]
+        res = xrt_rs.autotune(d_r, d_p, d_o, ctx=ctx, budget_ms=200.0, apply=True)
+        assert res["trials"] >= 1
+        out, st = run(ctx, rays, pix, "f32pr")
+        assert st["tuned"] == 1, (st, res)
+        exact = oracle.kahan_ld(rl, pl)
+        assert cases.rel_l2(out, exact) < PR_TOL
+        assert cases.rel_l2_intensity(out, exact) < PR_TOL
+        # The same bucket in a batch.
+        b = xrt_rs.Batch([(rays, pix)], path="f32pr", ctx=ctx)
+        outs = b.run()
+        assert b.plan(0)["tuned"] == 1
+        assert all(np.array_equal(x, y) for x, y in zip(outs[0], out))
+        b.close()
+        # Another bucket (100x the screen distance) is not tuned.
+        far = dict(pix, z=pix["z"] * 100.0)
+        _, st_far = run(ctx, rays, far, "f32pr")
+        assert st_far["tuned"] == 0
+        # Cache off: the defaults, bit for bit.
+        ctx.set_option("use_tuned", 0)
+        again, st2 = run(ctx, rays, pix, "f32pr")
+        assert st2["tuned"] == 0
+        assert all(np.array_equal(x, y) for x, y in zip(again, default))
+        ctx.set_option("use_tuned", 1)
+        ctx.set_option("clear_tuned", 1)
+        _, st3 = run(ctx, rays, pix, "f32pr")
+        assert st3["tuned"] == 0
+    finally:
+        ctx.close()

@@ -300,6 +300,7 @@ int xk_batch_solve_plan(const xk_batch* batch, size_t i, xk_solve_plan* out) {
     out->n_chunks = P.n_chunks;
     out->groups = P.groups;
     out->phase_bound_rad = P.phase_bound;
+    out->tuned = P.tuned ? 1 : 0;
     out->sweep = P.routed ? -1 : (P.fast ? (P.lin ? 2 : 1) : 0);
     out->one_polarization = !P.routed && P.one_pol;
     return XK_OK;

@@ -96,7 +96,8 @@ class XkBatchStats(ctypes.Structure):
 class XkSolvePlan(ctypes.Structure):
     _fields_ = [("path", ctypes.c_int), ("routed_reason", ctypes.c_int), ("n_tiles", ctypes.c_int),
                 ("n_chunks", ctypes.c_int), ("groups", ctypes.c_int), ("sweep", ctypes.c_int),
-                ("phase_bound_rad", ctypes.c_double), ("one_polarization", ctypes.c_int)]
+                ("phase_bound_rad", ctypes.c_double), ("one_polarization", ctypes.c_int),
+                ("tuned", ctypes.c_int)]
 
     def to_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
