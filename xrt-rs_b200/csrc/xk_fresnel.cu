@@ -142,6 +142,7 @@ constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + 2 * kFRayBytes + k
 
 struct FusedArgs {
     const double *rx, *rz, *er, *ei;
+    const StagedRay* staged;  // [ray_blocks * kFRays], from fresnel_stage_kernel
     size_t n;
     int ray_blocks, splits;
     const double *xp, *zp;
@@ -202,6 +203,43 @@ __device__ __forceinline__ uint32_t swap_halves(uint32_t v) { return __byte_perm
 
 __device__ __forceinline__ void producer_sync() {
     asm volatile("bar.sync 1, %0;" ::"n"(kFProdThreads) : "memory");
+}
+
+// Per-ray factors of the product, once per ray before the fused kernel: the
+// coordinates relative to the screen centre, the amplitude with the ray's own
+// phase, and the two rotations (phases reduced in FP64, sine and cosine to a
+// few ulp: their errors accumulate along a producer's rows). Rays past n
+// (the last block's padding) get zero amplitude.
+__global__ void __launch_bounds__(256)
+fresnel_stage_kernel(const double* __restrict__ rx, const double* __restrict__ rz,
+                     const double* __restrict__ er, const double* __restrict__ ei, size_t n,
+                     size_t n_pad, double ox, double oz, double a_turns, double dx, double dz,
+                     double inv_scale, StagedRay* __restrict__ out) {
+    const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (j >= n_pad) return;
+    StagedRay r;
+    r.pad0 = r.pad1 = 0.f;
+    if (j >= n) {
+        r.zr = r.xr = 0.0;
+        r.er = r.ei = 0.f;
+        r.ac = r.bc = 1.f;
+        r.as = r.bs = 0.f;
+    } else {
+        const double xr = rx[j] - ox, zr = rz[j] - oz;
+        r.zr = zr;
+        r.xr = xr;
+        const float2 ph = cis_turns_accurate(frac_turns(a_turns * (xr * xr + zr * zr)));
+        const float2 e = cmul(make_float2((float)(er[j] * inv_scale), (float)(ei[j] * inv_scale)), ph);
+        r.er = e.x;
+        r.ei = e.y;
+        const float2 ra = cis_turns_accurate(frac_turns(-2.0 * a_turns * dz * zr));
+        const float2 rb = cis_turns_accurate(frac_turns(-2.0 * a_turns * dx * xr));
+        r.ac = ra.x;
+        r.as = ra.y;
+        r.bc = rb.x;
+        r.bs = rb.y;
+    }
+    out[j] = r;
 }
 
 __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g) {
@@ -343,54 +381,28 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
         auto stage = [&](int buf) {
             return reinterpret_cast<StagedRay*>(rays_smem + buf * kFRayBytes);
         };
-        // Ray values of block `blk`. Threads 0..95 each handle one ray's part
-        // (0..31: coordinates and amplitude, 32..63: the z step, 64..95: the
-        // x step). `fetch` only issues the loads, so that they are in flight
-        // during the block's phasors; `put` reduces the phases in FP64 and
-        // stages the ray.
-        struct RawRay {
-            double x, z, er, ei;
-        };
-        auto fetch = [&](int blk, RawRay* v) {
-            const size_t j = (size_t)(rb0 + blk) * kFRays + (p & 31);
+        // The staged records of block `blk` (32 x 48 bytes, from
+        // fresnel_stage_kernel) are copied into shared memory by threads
+        // 0..95, 16 bytes each: `fetch` issues the load one block ahead, so
+        // that it is in flight during the block's phasors, `put` stores it.
+        auto fetch = [&](int blk, uint4* v) {
             if (p >= 96) return;
-            if (j >= g.n) {
-                *v = RawRay{g.ox, g.oz, 0.0, 0.0};
-                return;
-            }
-            *v = RawRay{__ldg(g.rx + j), __ldg(g.rz + j), __ldg(g.er + j), __ldg(g.ei + j)};
+            const uint4* src = reinterpret_cast<const uint4*>(g.staged + (size_t)(rb0 + blk) * kFRays);
+            *v = __ldg(src + p);
         };
-        auto put = [&](int buf, const RawRay& v) {
+        auto put = [&](int buf, const uint4& v) {
             if (p >= 96) return;
-            StagedRay& sr = stage(buf)[p & 31];
-            const double xr = v.x - g.ox, zr = v.z - g.oz;
-            if (p < 32) {
-                const float2 ph = cis_turns_accurate(frac_turns(g.a_turns * (xr * xr + zr * zr)));
-                const float2 a = make_float2((float)(v.er * g.inv_scale), (float)(v.ei * g.inv_scale));
-                const float2 e = cmul(a, ph);
-                sr.zr = zr;
-                sr.xr = xr;
-                sr.er = e.x;
-                sr.ei = e.y;
-            } else if (p < 64) {
-                const float2 rot = cis_turns_accurate(frac_turns(-2.0 * g.a_turns * g.dz * zr));
-                sr.ac = rot.x;
-                sr.as = rot.y;
-            } else {
-                const float2 rot = cis_turns_accurate(frac_turns(-2.0 * g.a_turns * g.dx * xr));
-                sr.bc = rot.x;
-                sr.bs = rot.y;
-            }
+            reinterpret_cast<uint4*>(stage(buf))[p] = v;
         };
         if (nrb > 0) {
-            RawRay v;
+            uint4 v;
             fetch(0, &v);
             put(0, v);
         }
         producer_sync();
         for (int i = 0; i < nrb; ++i) {
             const int s = i % kFStages, rbuf = i & 1;
-            RawRay nxt{g.ox, g.oz, 0.0, 0.0};
+            uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
             if (i + 1 < nrb) fetch(i + 1, &nxt);  // in flight during this block
             // This thread's 4 rays: seed phasors at the first row and the
             // per-row rotation.
@@ -594,7 +606,18 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     XK_CUDA_TRY(attr_err);
     int* d_err = ws.ctrl.as<int>();
     XK_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
+    // Per-ray factors, one record per ray of every block (padding included).
+    const size_t n_pad = (size_t)sh.ray_blocks * kFRays;
+    XK_TRY(ws.staged.ensure(n_pad * sizeof(StagedRay)));
+    const double dxs = (in.x_max - in.x_min) / (double)(nx > 1 ? nx - 1 : 1);
+    const double dzs = (in.z_max - in.z_min) / (double)(nz > 1 ? nz - 1 : 1);
+    fresnel_stage_kernel<<<grid_1d(n_pad, 256), 256, 0, stream>>>(
+        in.rx, in.rz, in.er, in.ei, n, n_pad, ox, oz, pre * kInv2Pi, dxs, dzs, 1.0 / in.max_amp,
+        ws.staged.as<StagedRay>());
+    XK_CUDA_TRY(cudaGetLastError());
+    rep->kernels += 1;
     FusedArgs fa;
+    fa.staged = ws.staged.as<StagedRay>();
     fa.rx = in.rx;
     fa.rz = in.rz;
     fa.er = in.er;
@@ -610,8 +633,8 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     fa.inv_scale = 1.0 / in.max_amp;
     fa.ox = ox;
     fa.oz = oz;
-    fa.dx = (in.x_max - in.x_min) / (double)(nx > 1 ? nx - 1 : 1);
-    fa.dz = (in.z_max - in.z_min) / (double)(nz > 1 ? nz - 1 : 1);
+    fa.dx = dxs;
+    fa.dz = dzs;
     fa.partial = ws.partial.as<double>();
     fa.m_pad = (int)sh.m_pad;
     fa.n_pad = (int)sh.n_pad;

@@ -3,16 +3,16 @@
 // The phase-reduced pair kernel is bound by these two pipes, not by HBM or
 // the tensor cores, so its roofline needs their peak rates on this part.
 // Two kernels measure them with every SM busy:
-//   * ffma2_probe: 8 independent f32x2 FMA chains per thread, 8 warps per
-//     block, enough blocks for 32 warps per SM (an f32x2 FMA counts as two
-//     lane operations);
+//   * ffma2_probe: 8 independent f32x2 FMA chains per thread, 32 warps per
+//     SM (an f32x2 FMA counts as two lane operations);
 //   * mufu_probe: 8 independent chains of sin.approx / cos.approx per thread
 //     (each MUFU result counts once; the range multiply before each one runs
 //     on the FMA pipe, far below its rate).
-// Each block reads clock64 on entry and exit; with every block of an SM
-// resident at once, a block's cycle count is the SM's, so the rates come out
-// per SM clock, independent of the clock the GPU happened to run at. CUDA
-// events give the wall time, and cycles over time the SM clock seen.
+// One block of 1024 threads per SM (its shared-memory request keeps a second
+// block off the SM), so a block's clock64 cycle count between entry and exit
+// is its SM's: the rates come out per SM clock, independent of the clock the
+// GPU happened to run at. CUDA events give the wall time, and cycles over
+// time the SM clock seen.
 
 #include <algorithm>
 #include <vector>
@@ -22,13 +22,12 @@
 namespace xk {
 namespace {
 
-constexpr int kProbeThreads = 256;
-constexpr int kProbeBlocksPerSm = 4;
+constexpr int kProbeThreads = 1024;
+constexpr int kProbeBlocksPerSm = 1;
 constexpr int kProbeChains = 8;
-// Dynamic shared memory per block that caps residency at kProbeBlocksPerSm
-// blocks per SM (5 x 48 KB exceeds the SM's 228 KB), so that a grid of
-// kProbeBlocksPerSm blocks per SM is resident all at once, evenly.
-constexpr int kProbeSmem = 48 * 1024;
+// Dynamic shared memory per block: more than half the SM's 228 KB, so every
+// SM holds exactly one block of the num_sms-block grid.
+constexpr int kProbeSmem = 120 * 1024;
 
 __global__ void __launch_bounds__(kProbeThreads)
 ffma2_probe(int iters, float seed, float* __restrict__ sink, long long* __restrict__ cycles) {
@@ -94,8 +93,8 @@ struct ProbeRun {
     double clk_mhz = 0.0;
 };
 
-// Runs `kern` on num_sms * kProbeBlocksPerSm blocks; ops_per_block lane
-// operations per block; the rate uses the median block's cycle count.
+// Runs `kern` on num_sms blocks (one per SM); ops_per_block lane operations
+// per block; the rate uses the median block's cycle count.
 template <class K>
 Status run_probe(K kern, int iters, double ops_per_block, int num_sms, cudaStream_t s,
                  DevBuf& scratch, ProbeRun* out) {
@@ -139,7 +138,7 @@ extern "C" int xk_probe_pipes(xk_ctx* ctx, xk_pipe_peaks* out) {
     xk::DevBuf scratch;
     xk::ProbeRun f, m;
     // ~20-50 ms per probe at B200 clocks.
-    const int fma_iters = 1 << 15, mufu_iters = 1 << 13;
+    const int fma_iters = 1 << 13, mufu_iters = 1 << 11;
     const double fma_ops = (double)fma_iters * 4 * xk::kProbeChains * 2 * xk::kProbeThreads;
     const double mufu_ops = (double)mufu_iters * 2 * xk::kProbeChains * xk::kProbeThreads;
     xk::Status st = xk::run_probe(xk::ffma2_probe, fma_iters, fma_ops, ctx->num_sms, ctx->stream,
