@@ -112,6 +112,8 @@ typedef struct xk_stats {
     int one_polarization;    /* F32PR: 1 if every ray had ray 0's polarization, so the kernel
                                 summed one amplitude column and Ep = (ep_0 / es_0) Es */
     int tuned;               /* F32PR: 1 if the solve used autotuned settings of its bucket */
+    int folded;              /* F32PR: 1 if the kernel folded each point's base phase into the
+                                per-pair phase (near field) */
 } xk_stats;
 
 /* ---- context ------------------------------------------------------------ */

@@ -94,6 +94,7 @@ pub struct xk_stats {
     pub sweep: c_int,
     pub one_polarization: c_int,
     pub tuned: c_int,
+    pub folded: c_int,
 }
 
 #[repr(C)]

@@ -65,9 +65,12 @@ def test_one_polarization_matches_two_columns_and_oracle(pol_ctx, oracle, name):
     two, st2 = run(pol_ctx, rays, pix)
     assert st2["one_polarization"] == 0
     if name != "es_zero":
-        # The summed column is es: its FP32 operations are those of the
-        # two-column kernel's Es sum, so Es agrees bit for bit.
-        assert np.array_equal(one[0], two[0]) and np.array_equal(one[1], two[1])
+        # The summed column is es. The one-column far-field kernel carries it
+        # in polar form (its phase joins the pair's residual phase), so Es
+        # agrees with the two-column kernel's to FP32 rounding, not bitwise.
+        es1 = one[0] + 1j * one[1]
+        es2 = two[0] + 1j * two[1]
+        assert np.linalg.norm(es1 - es2) / np.linalg.norm(es2) < 1e-6
     ref = oracle.kahan_f64(*cases.as_lists(rays, pix))
     assert cases.rel_l2(one, ref) < PR_TOL
     assert cases.rel_l2(one, two) < 1e-6

@@ -121,6 +121,7 @@ xk::Status run_solve(xk_ctx* ctx, const xk::RaysDev& rays, size_t n_rays, const 
         ctx->last_dist_mm = P.dist_mm;
         if (stats) {
             stats->tuned = P.tuned ? 1 : 0;
+            stats->folded = !P.routed && P.fold ? 1 : 0;
             stats->n_tiles = P.n_tiles;
             stats->n_chunks = P.n_chunks;
             stats->n_items = (long long)P.n_tiles * P.groups;

@@ -71,6 +71,7 @@ class XkStats(ctypes.Structure):
         ("sweep", ctypes.c_int),
         ("one_polarization", ctypes.c_int),
         ("tuned", ctypes.c_int),
+        ("folded", ctypes.c_int),
     ]
 
     def to_dict(self):
