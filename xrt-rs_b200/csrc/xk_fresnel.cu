@@ -26,11 +26,11 @@
 //   product runs on Z[iz][j] = exp(-2 i a z_iz z_j) and
 //   W[ix][j] = es'_j exp(-2 i a x_ix x_j), whose phases are linear in the
 //   screen index. One fused kernel computes it on the tensor cores without
-//   ever writing A or B to memory: per block of 32 rays, eight producer warps
-//   form the CTA's A (128 z rows) and B (128 x points, 256 rows) tiles; a
-//   thread owns 4 rays x 8 consecutive rows, seeds each ray's phasor from an
+//   ever writing A or B to memory: per block of 32 rays, sixteen producer
+//   warps form the CTA's A (128 z rows) and B (128 x points, 256 rows) tiles;
+//   a thread owns 4 rays x 4 consecutive rows, seeds each ray's phasor from an
 //   FP64-reduced phase at its first row and steps it along the rows by one
-//   complex rotation exp(-2 i a dz z_j) (so 7 of 8 phasors cost a complex
+//   complex rotation exp(-2 i a dz z_j) (so 3 of 4 phasors cost a complex
 //   multiply instead of a sine and cosine), splits each phasor into f16
 //   hi + lo parts and stores them in the 128-byte-swizzled K-major layout;
 //   one thread issues tcgen05.mma kind::f16 (f32 accumulation in tensor
@@ -121,7 +121,7 @@ constexpr uint32_t kFA = 128 * 64 * 2;           // one A tile (hi or lo): 128 r
 constexpr uint32_t kFB = 256 * 64 * 2;           // one B tile: 256 rows x 128 B
 constexpr uint32_t kFStage = 2 * kFA + 2 * kFB;  // A_hi | A_lo | B_hi | B_lo
 constexpr int kFEpiThreads = 128;                // warps 1..4
-constexpr int kFProdThreads = 256;               // warps 5..12
+constexpr int kFProdThreads = 512;               // warps 5..20
 constexpr int kFThreads = 32 + kFEpiThreads + kFProdThreads;
 constexpr int kFSeg = 20;                        // ray blocks (60 K blocks) per f32 segment
 constexpr int kFN = 256;                         // accumulator columns (N of the UMMA)
@@ -135,7 +135,8 @@ struct __align__(16) StagedRay {
 };
 static_assert(sizeof(StagedRay) == 48, "staged ray is 48 bytes");
 constexpr uint32_t kFRayBytes = kFRays * sizeof(StagedRay);
-constexpr int kFRowsPerThread = 8;  // consecutive rows a producer steps by rotation
+constexpr int kFRowsPerThread = 4;  // consecutive rows a producer steps by rotation
+static_assert(kFProdThreads / 2 / 8 * kFRowsPerThread == 128, "producers cover the 128-row tiles");
 // Epilogue transpose buffers: per epilogue warp 32 x 33 floats.
 constexpr uint32_t kFEpiBytes = 4 * 32 * 33 * 4;
 constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + 2 * kFRayBytes + kFEpiBytes + 256;
@@ -365,14 +366,15 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             mbar_arrive(&acc_empty[b]);
         }
     } else {
-        // Producers. Threads 0..127 build A, 128..255 build B: thread q owns
-        // the 4 rays of 16-byte chunk c = q % 8 and the 8 consecutive rows
-        // (A: screen z rows, B: screen x points) 8 (q / 8) .. + 7 of the tile.
+        // Producers. Threads 0..255 build A, 256..511 build B: thread q owns
+        // the 4 rays of 16-byte chunk c = q % 8 and the kFRowsPerThread
+        // consecutive rows (A: screen z rows, B: screen x points) starting at
+        // kFRowsPerThread (q / 8) of the tile.
         // Per block it seeds each ray's phasor at its first row from the
         // FP64-reduced phase and rotates it row by row.
         const int p = threadIdx.x - 160;
-        const bool is_b = p >= 128;
-        const int q = p & 127, c = q & 7, r0 = (q >> 3) * kFRowsPerThread;
+        const bool is_b = p >= kFProdThreads / 2;
+        const int q = p % (kFProdThreads / 2), c = q & 7, r0 = (q >> 3) * kFRowsPerThread;
         const size_t first = (size_t)(is_b ? nt : mt) * 128 + r0;
         const size_t lim = is_b ? g.nx : g.nz;
         // kappa of the first row, in turns per mm: -2 a (p0 - o).
