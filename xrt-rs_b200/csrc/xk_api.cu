@@ -70,7 +70,6 @@ void destroy_ctx(xk_ctx* ctx) {
     ctx->fresnel.coords.release();
     ctx->fresnel.partial.release();
     ctx->fresnel.ctrl.release();
-    ctx->fresnel.staged.release();
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

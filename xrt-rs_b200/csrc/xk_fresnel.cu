@@ -19,20 +19,11 @@
 //       C[iz][2 ix + c] = sum_k A[iz][k] B[2 ix + c][k],
 //       A[iz][2j] = Re Z, A[iz][2j+1] = Im Z,
 //       B[2ix][2j] = Re W, B[2ix][2j+1] = -Im W, B[2ix+1][2j] = Im W, B[2ix+1][2j+1] = Re W,
-//   with W = es X / max|es|. With p and r taken relative to the screen
-//   centre, (p - r)^2 = p^2 - 2 p r + r^2, so the row factors exp(i a x^2),
-//   exp(i a z^2) leave the sum (the final reduction applies them in FP64)
-//   and the ray factor exp(i a (x_j^2 + z_j^2)) joins the amplitude: the
-//   product runs on Z[iz][j] = exp(-2 i a z_iz z_j) and
-//   W[ix][j] = es'_j exp(-2 i a x_ix x_j), whose phases are linear in the
-//   screen index. One fused kernel computes it on the tensor cores without
-//   ever writing A or B to memory: per block of 32 rays, sixteen producer
-//   warps form the CTA's A (128 z rows) and B (128 x points, 256 rows) tiles;
-//   a thread owns 4 rays x 4 consecutive rows, seeds each ray's phasor from an
-//   FP64-reduced phase at its first row and steps it along the rows by one
-//   complex rotation exp(-2 i a dz z_j) (so 3 of 4 phasors cost a complex
-//   multiply instead of a sine and cosine), splits each phasor into f16
-//   hi + lo parts and stores them in the 128-byte-swizzled K-major layout;
+//   with W = es X / max|es|. One fused kernel computes it on the tensor
+//   cores without ever writing A or B to memory: per block of 32 rays, eight
+//   producer warps form the CTA's A (128 z rows) and B (128 x points, 256
+//   rows) tiles from FP64 phases, split each phasor into f16 hi + lo parts
+//   and store them in shared memory in the 128-byte-swizzled K-major layout;
 //   one thread issues tcgen05.mma kind::f16 (f32 accumulation in tensor
 //   memory) for A_hi B_hi + A_hi B_lo + A_lo B_hi, which keeps ~2^-21 of each
 //   phasor; four epilogue warps drain the accumulator into an FP64 partial
@@ -121,29 +112,20 @@ constexpr uint32_t kFA = 128 * 64 * 2;           // one A tile (hi or lo): 128 r
 constexpr uint32_t kFB = 256 * 64 * 2;           // one B tile: 256 rows x 128 B
 constexpr uint32_t kFStage = 2 * kFA + 2 * kFB;  // A_hi | A_lo | B_hi | B_lo
 constexpr int kFEpiThreads = 128;                // warps 1..4
-constexpr int kFProdThreads = 512;               // warps 5..20
+constexpr int kFProdThreads = 256;               // warps 5..12
 constexpr int kFThreads = 32 + kFEpiThreads + kFProdThreads;
 constexpr int kFSeg = 20;                        // ray blocks (60 K blocks) per f32 segment
 constexpr int kFN = 256;                         // accumulator columns (N of the UMMA)
-// Ray staging (two blocks), one StagedRay per ray.
-struct __align__(16) StagedRay {
-    double zr, xr;   // coordinates relative to the screen centre [mm]
-    float er, ei;    // es exp(2 pi i a_turns (xr^2 + zr^2)) / max|es|
-    float ac, as;    // exp(-2 pi i 2 a_turns dz zr): one row step of Z
-    float bc, bs;    // exp(-2 pi i 2 a_turns dx xr): one point step of W
-    float pad0, pad1;
-};
-static_assert(sizeof(StagedRay) == 48, "staged ray is 48 bytes");
-constexpr uint32_t kFRayBytes = kFRays * sizeof(StagedRay);
-constexpr int kFRowsPerThread = 4;  // consecutive rows a producer steps by rotation
-static_assert(kFProdThreads / 2 / 8 * kFRowsPerThread == 128, "producers cover the 128-row tiles");
+// Ray staging (two blocks), per ray 8 floats: x hi, x lo, frac(a x^2), z hi,
+// z lo, frac(a z^2) (coordinates relative to the screen centre) and the
+// scaled amplitude.
+constexpr uint32_t kFRayBytes = kFRays * 32;
 // Epilogue transpose buffers: per epilogue warp 32 x 33 floats.
 constexpr uint32_t kFEpiBytes = 4 * 32 * 33 * 4;
 constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + 2 * kFRayBytes + kFEpiBytes + 256;
 
 struct FusedArgs {
     const double *rx, *rz, *er, *ei;
-    const StagedRay* staged;  // [ray_blocks * kFRays], from fresnel_stage_kernel
     size_t n;
     int ray_blocks, splits;
     const double *xp, *zp;
@@ -151,7 +133,6 @@ struct FusedArgs {
     double a_turns;    // k / (2 d) / (2 pi)
     double inv_scale;  // 1 / max|es|
     double ox, oz;     // origin of the phase split (screen centre)
-    double dx, dz;     // screen steps (x_max - x_min) / max(nx - 1, 1), same in z
     double* partial;   // [splits][m_pad][n_pad]
     int m_pad, n_pad;
     int* err;
@@ -163,29 +144,45 @@ __device__ __forceinline__ uint32_t sw128(uint32_t r, uint32_t c) {
     return r * 128u + ((c ^ (r & 7u)) << 4);
 }
 
+// Phase split. With p, r relative to the screen centre the phase in turns is
+//     t = a (p - r)^2 = P(p) + kappa(p) r + R(r),
+//     P = frac(a p^2), R = frac(a r^2), kappa = -2 a p,
+// where P and R are reduced in FP64 once per screen row and per ray. The
+// cross term kappa r (up to 2^21 turns, checked on the host) is formed
+// exactly in FP32 from hi/lo splits of kappa and r: the rounded product
+// kh*rh, its FMA error term, and the two small cross products; its integer
+// part drops out and the fractional remainder keeps ~1e-7 turn.
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: (x + kMagic) - kMagic = rint(x), |x| < 2^22
+
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-// Fractional part of an FP64 phase in turns, as a float in [-1/2, 1/2].
-__device__ __forceinline__ float frac_turns(double t) { return (float)(t - rint(t)); }
-
-// (c, s) = (cos, sin) of 2 pi f for |f| <= 1/2, to a few ulp (per ray, once
-// per block: the rotation factors must be accurate, their errors add up
-// along a thread's rows).
-__device__ __forceinline__ float2 cis_turns_accurate(float f) {
-    float sn, cs;
-    sincospif(2.f * f, &sn, &cs);
-    return make_float2(cs, sn);
+// The same for a row of A (.x) and a row of B (.y) at once on sm_100's packed
+// f32x2 instructions, with the operation sequence and roundings of the scalar
+// form: p1 = kh rh rounded, e1 = its FMA error, f1 = p1 - rint(p1),
+// t = (pr + f1) + (kh rl + kl rh + e1), result t - rint(t). rint is the
+// magic-number rounding (exact and sign-symmetric for |x| < 2^22), and the
+// product is carried negated (khn = -kh) so that every step is one packed
+// FMA, multiply or add; a - b is formed as fma(b, -1, a).
+__device__ __forceinline__ float2 pair_turns2(float2 kh, float2 khn, float2 kl, float2 pr,
+                                              float2 rh, float2 rl) {
+    const float2 m = f2(kMagic), mn = f2(-kMagic), one_n = f2(-1.f);
+    const float2 p1n = __fmul2_rn(khn, rh);                          // -p1
+    const float2 e1 = __ffma2_rn(kh, rh, p1n);                       // kh rh - p1
+    const float2 r1 = __fadd2_rn(__fadd2_rn(p1n, m), mn);            // rint(-p1)
+    const float2 f1n = __ffma2_rn(r1, one_n, p1n);                   // -f1
+    float2 sm = __ffma2_rn(kh, rl, e1);
+    sm = __ffma2_rn(kl, rh, sm);
+    const float2 t = __fadd2_rn(__ffma2_rn(f1n, one_n, pr), sm);    // (pr + f1) + sm
+    const float2 rt = __fadd2_rn(__fadd2_rn(t, m), mn);
+    return __ffma2_rn(rt, one_n, t);                                 // t - rint(t)
 }
 
-// (c, s) of 2 pi f, |f| <= 1/2, on the SFU (~4e-7 absolute): the seeds.
-__device__ __forceinline__ float2 cis_turns_fast(float f) {
-    float sn, cs;
-    __sincosf(6.28318530717958647692f * f, &sn, &cs);
-    return make_float2(cs, sn);
-}
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+// hi/lo float split of a double and frac(a v^2) as a float.
+__device__ __forceinline__ void split_coord(double v, double a, float* hi, float* lo, float* fr) {
+    *hi = (float)v;
+    *lo = (float)(v - (double)*hi);
+    const double t = (a * v) * v;
+    *fr = (float)(t - rint(t));
 }
 
 // (a, b) -> f16x2 hi (round to nearest) and f16x2 lo = (a, b) - hi.
@@ -204,43 +201,6 @@ __device__ __forceinline__ uint32_t swap_halves(uint32_t v) { return __byte_perm
 
 __device__ __forceinline__ void producer_sync() {
     asm volatile("bar.sync 1, %0;" ::"n"(kFProdThreads) : "memory");
-}
-
-// Per-ray factors of the product, once per ray before the fused kernel: the
-// coordinates relative to the screen centre, the amplitude with the ray's own
-// phase, and the two rotations (phases reduced in FP64, sine and cosine to a
-// few ulp: their errors accumulate along a producer's rows). Rays past n
-// (the last block's padding) get zero amplitude.
-__global__ void __launch_bounds__(256)
-fresnel_stage_kernel(const double* __restrict__ rx, const double* __restrict__ rz,
-                     const double* __restrict__ er, const double* __restrict__ ei, size_t n,
-                     size_t n_pad, double ox, double oz, double a_turns, double dx, double dz,
-                     double inv_scale, StagedRay* __restrict__ out) {
-    const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (j >= n_pad) return;
-    StagedRay r;
-    r.pad0 = r.pad1 = 0.f;
-    if (j >= n) {
-        r.zr = r.xr = 0.0;
-        r.er = r.ei = 0.f;
-        r.ac = r.bc = 1.f;
-        r.as = r.bs = 0.f;
-    } else {
-        const double xr = rx[j] - ox, zr = rz[j] - oz;
-        r.zr = zr;
-        r.xr = xr;
-        const float2 ph = cis_turns_accurate(frac_turns(a_turns * (xr * xr + zr * zr)));
-        const float2 e = cmul(make_float2((float)(er[j] * inv_scale), (float)(ei[j] * inv_scale)), ph);
-        r.er = e.x;
-        r.ei = e.y;
-        const float2 ra = cis_turns_accurate(frac_turns(-2.0 * a_turns * dz * zr));
-        const float2 rb = cis_turns_accurate(frac_turns(-2.0 * a_turns * dx * xr));
-        r.ac = ra.x;
-        r.as = ra.y;
-        r.bc = rb.x;
-        r.bs = rb.y;
-    }
-    out[j] = r;
 }
 
 __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g) {
@@ -366,91 +326,113 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             mbar_arrive(&acc_empty[b]);
         }
     } else {
-        // Producers. Threads 0..255 build A, 256..511 build B: thread q owns
-        // the 4 rays of 16-byte chunk c = q % 8 and the kFRowsPerThread
-        // consecutive rows (A: screen z rows, B: screen x points) starting at
-        // kFRowsPerThread (q / 8) of the tile.
-        // Per block it seeds each ray's phasor at its first row from the
-        // FP64-reduced phase and rotates it row by row.
+        // Producers: thread p owns A row r (screen z index mt*128 + r) and B
+        // rows 2r, 2r+1 (screen x index nt*128 + r) for rays 16h .. 16h+15 of
+        // each block (h = p / 128), i.e. 16-byte chunks 4h .. 4h+3 of its rows.
+        // The block's rays are staged in shared memory one block ahead by
+        // threads 0..95 (rx, rz, scaled amplitude).
         const int p = threadIdx.x - 160;
-        const bool is_b = p >= kFProdThreads / 2;
-        const int q = p % (kFProdThreads / 2), c = q & 7, r0 = (q >> 3) * kFRowsPerThread;
-        const size_t first = (size_t)(is_b ? nt : mt) * 128 + r0;
-        const size_t lim = is_b ? g.nx : g.nz;
-        // kappa of the first row, in turns per mm: -2 a (p0 - o).
-        const double p0 = first < lim ? (is_b ? g.xp[first] - g.ox : g.zp[first] - g.oz) : 0.0;
-        const double kappa0 = -2.0 * g.a_turns * p0;
-        auto stage = [&](int buf) {
-            return reinterpret_cast<StagedRay*>(rays_smem + buf * kFRayBytes);
+        const int h = p >> 7, r = p & 127;
+        const size_t iz = (size_t)mt * 128 + r, ix = (size_t)nt * 128 + r;
+        const bool va = iz < g.nz, vb = ix < g.nx;
+        // Per-row terms: kappa = -2 a p (hi, lo) and P = frac(a p^2).
+        float kzh = 0.f, kzl = 0.f, pz = 0.f, kxh = 0.f, kxl = 0.f, px = 0.f;
+        {
+            const double zr = va ? g.zp[iz] - g.oz : 0.0, xr = vb ? g.xp[ix] - g.ox : 0.0;
+            float unused;
+            split_coord(-2.0 * g.a_turns * zr, 0.0, &kzh, &kzl, &unused);
+            split_coord(-2.0 * g.a_turns * xr, 0.0, &kxh, &kxl, &unused);
+            float h0, l0;
+            split_coord(zr, g.a_turns, &h0, &l0, &pz);
+            split_coord(xr, g.a_turns, &h0, &l0, &px);
+        }
+        const float2 kh2 = make_float2(kzh, kxh), khn2 = make_float2(-kzh, -kxh),
+                     kl2 = make_float2(kzl, kxl), pp2 = make_float2(pz, px);
+        auto stage = [&](int buf) { return reinterpret_cast<float4*>(rays_smem + buf * kFRayBytes); };
+        // Ray values of block `blk` (threads 0..31, one ray each). `fetch`
+        // only issues the loads, so that they are in flight during the
+        // block's phasors; `put` splits them and stages them as (z, x) pairs
+        // for the packed phase: {zh, xh, zl, xl}, {zf, xf, es_re, es_im}
+        // (amplitude scaled).
+        struct RawRay {
+            double x, z, er, ei;
         };
-        // The staged records of block `blk` (32 x 48 bytes, from
-        // fresnel_stage_kernel) are copied into shared memory by threads
-        // 0..95, 16 bytes each: `fetch` issues the load one block ahead, so
-        // that it is in flight during the block's phasors, `put` stores it.
-        auto fetch = [&](int blk, uint4* v) {
-            if (p >= 96) return;
-            const uint4* src = reinterpret_cast<const uint4*>(g.staged + (size_t)(rb0 + blk) * kFRays);
-            *v = __ldg(src + p);
+        auto fetch = [&](int blk, RawRay* v) {
+            const size_t j = (size_t)(rb0 + blk) * kFRays + p;
+            if (p >= 32) return;
+            if (j >= g.n) {
+                *v = RawRay{g.ox, g.oz, 0.0, 0.0};
+                return;
+            }
+            *v = RawRay{__ldg(g.rx + j), __ldg(g.rz + j), __ldg(g.er + j), __ldg(g.ei + j)};
         };
-        auto put = [&](int buf, const uint4& v) {
-            if (p >= 96) return;
-            reinterpret_cast<uint4*>(stage(buf))[p] = v;
+        auto put = [&](int buf, const RawRay& v) {
+            if (p < 32) {
+                float xh, xl, xf, zh, zl, zf;
+                split_coord(v.x - g.ox, g.a_turns, &xh, &xl, &xf);
+                split_coord(v.z - g.oz, g.a_turns, &zh, &zl, &zf);
+                stage(buf)[2 * p] = make_float4(zh, xh, zl, xl);
+                stage(buf)[2 * p + 1] = make_float4(zf, xf, (float)(v.er * g.inv_scale),
+                                                    (float)(v.ei * g.inv_scale));
+            }
         };
         if (nrb > 0) {
-            uint4 v;
+            RawRay v;
             fetch(0, &v);
             put(0, v);
         }
         producer_sync();
         for (int i = 0; i < nrb; ++i) {
             const int s = i % kFStages, rbuf = i & 1;
-            uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
+            RawRay nxt{g.ox, g.oz, 0.0, 0.0};
             if (i + 1 < nrb) fetch(i + 1, &nxt);  // in flight during this block
-            // This thread's 4 rays: seed phasors at the first row and the
-            // per-row rotation.
-            const StagedRay* sr = stage(rbuf);
-            float2 ph[4], rot[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const StagedRay& ry = sr[4 * c + u];
-                const double coord = is_b ? ry.xr : ry.zr;
-                const float2 seed = cis_turns_fast(frac_turns(kappa0 * coord));
-                ph[u] = is_b ? cmul(make_float2(ry.er, ry.ei), seed) : seed;
-                rot[u] = is_b ? make_float2(ry.bc, ry.bs) : make_float2(ry.ac, ry.as);
-            }
             if (!mbar_wait(&empty[s], ((uint32_t)(i / kFStages) & 1u) ^ 1u, g.wait_limit)) *flag = 1;
             unsigned char* base = tiles + (size_t)s * kFStage;
-#pragma unroll 2
-            for (int k = 0; k < kFRowsPerThread; ++k) {
-                const int row = r0 + k;
-                const bool valid = first + k < lim;
-                uint32_t hi[4], lo[4];
+            const float4* sr = stage(rbuf);
+#pragma unroll 1
+            for (int cc = 0; cc < 4; ++cc) {
+                const int c = 4 * h + cc;
+                uint32_t ah[4], al[4], bh[4], bl[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    split16x2(valid ? ph[u].x : 0.f, valid ? ph[u].y : 0.f, &hi[u], &lo[u]);
-                    ph[u] = cmul(ph[u], rot[u]);
+                for (int jj = 0; jj < 4; ++jj) {
+                    const int j = 4 * c + jj;
+                    const float4 v0 = sr[2 * j], v1 = sr[2 * j + 1];
+                    // Phase in turns of the A row (.x) and the B row (.y).
+                    const float2 t = pair_turns2(kh2, khn2, kl2,
+                                                 __fadd2_rn(pp2, make_float2(v1.x, v1.y)),
+                                                 make_float2(v0.x, v0.y), make_float2(v0.z, v0.w));
+                    const float2 th = __fmul2_rn(t, f2(6.28318530717958647692f));
+                    float ca, sa, cb, sb, wr = 0.f, wi = 0.f;
+                    __sincosf(th.x, &sa, &ca);
+                    __sincosf(th.y, &sb, &cb);
+                    if (!va) ca = sa = 0.f;
+                    if (vb) {
+                        wr = v1.z * cb - v1.w * sb;
+                        wi = v1.z * sb + v1.w * cb;
+                    }
+                    split16x2(ca, sa, &ah[jj], &al[jj]);
+                    split16x2(wr, wi, &bh[jj], &bl[jj]);
                 }
-                if (!is_b) {
-                    // A row: (Re Z, Im Z) per ray.
-                    *reinterpret_cast<uint4*>(base + sw128(row, c)) =
-                        make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                    *reinterpret_cast<uint4*>(base + kFA + sw128(row, c)) =
-                        make_uint4(lo[0], lo[1], lo[2], lo[3]);
-                } else {
-                    // B rows 2 row: (Re W, -Im W), 2 row + 1: (Im W, Re W).
-                    unsigned char* bhi = base + 2 * kFA;
-                    unsigned char* blo = bhi + kFB;
-                    *reinterpret_cast<uint4*>(bhi + sw128(2 * row, c)) =
-                        make_uint4(neg_hi(hi[0]), neg_hi(hi[1]), neg_hi(hi[2]), neg_hi(hi[3]));
-                    *reinterpret_cast<uint4*>(bhi + sw128(2 * row + 1, c)) =
-                        make_uint4(swap_halves(hi[0]), swap_halves(hi[1]), swap_halves(hi[2]),
-                                   swap_halves(hi[3]));
-                    *reinterpret_cast<uint4*>(blo + sw128(2 * row, c)) =
-                        make_uint4(neg_hi(lo[0]), neg_hi(lo[1]), neg_hi(lo[2]), neg_hi(lo[3]));
-                    *reinterpret_cast<uint4*>(blo + sw128(2 * row + 1, c)) =
-                        make_uint4(swap_halves(lo[0]), swap_halves(lo[1]), swap_halves(lo[2]),
-                                   swap_halves(lo[3]));
-                }
+                // A row: (Re Z, Im Z); B rows 2r: (Re W, -Im W), 2r+1: (Im W, Re W).
+                *reinterpret_cast<uint4*>(base + sw128(r, c)) = make_uint4(ah[0], ah[1], ah[2], ah[3]);
+                *reinterpret_cast<uint4*>(base + kFA + sw128(r, c)) =
+                    make_uint4(al[0], al[1], al[2], al[3]);
+                unsigned char* bhi = base + 2 * kFA;
+                unsigned char* blo = bhi + kFB;
+                // Rows 2r and 2r+1. Eight consecutive threads' stores to even
+                // rows meet four swizzle phases (a 2-way conflict); ordering
+                // the two stores per thread to spread them cost 16 selects
+                // per chunk and was 1.5 % slower overall.
+                const uint4 e0h = make_uint4(neg_hi(bh[0]), neg_hi(bh[1]), neg_hi(bh[2]), neg_hi(bh[3]));
+                const uint4 e1h = make_uint4(swap_halves(bh[0]), swap_halves(bh[1]),
+                                             swap_halves(bh[2]), swap_halves(bh[3]));
+                const uint4 e0l = make_uint4(neg_hi(bl[0]), neg_hi(bl[1]), neg_hi(bl[2]), neg_hi(bl[3]));
+                const uint4 e1l = make_uint4(swap_halves(bl[0]), swap_halves(bl[1]),
+                                             swap_halves(bl[2]), swap_halves(bl[3]));
+                *reinterpret_cast<uint4*>(bhi + sw128(2 * r, c)) = e0h;
+                *reinterpret_cast<uint4*>(bhi + sw128(2 * r + 1, c)) = e1h;
+                *reinterpret_cast<uint4*>(blo + sw128(2 * r, c)) = e0l;
+                *reinterpret_cast<uint4*>(blo + sw128(2 * r + 1, c)) = e1l;
             }
             // Make the generic-proxy stores visible to the tensor cores, then
             // one arrival per warp.
@@ -512,28 +494,21 @@ __global__ void __launch_bounds__(256) ray_bounds_kernel(const double* __restric
     }
 }
 
-// The product's row factors are applied here in FP64:
-// U = scale exp(2 pi i a_turns ((x - ox)^2 + (z - oz)^2)) C.
 __global__ void reduce_kernel(const double* __restrict__ partial, int splits, int m_pad, int n_pad,
-                              size_t nz, size_t nx, double scale, const double* __restrict__ xp,
-                              const double* __restrict__ zp, double ox, double oz, double a_turns,
-                              double* __restrict__ acc_re, double* __restrict__ acc_im, int first) {
+                              size_t nz, size_t nx, double scale, double* __restrict__ acc_re,
+                              double* __restrict__ acc_im, int first) {
     const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (idx >= nz * nx) return;
     const size_t iz = idx / nx, ix = idx - iz * nx;
-    double cr = 0.0, ci = 0.0;
+    double re = 0.0, im = 0.0;
     for (int s = 0; s < splits; ++s) {
         const double2 v = *reinterpret_cast<const double2*>(
             partial + ((size_t)s * m_pad + iz) * n_pad + 2 * ix);
-        cr += v.x;
-        ci += v.y;
+        re += v.x;
+        im += v.y;
     }
-    const double x = xp[ix] - ox, z = zp[iz] - oz;
-    const double t = a_turns * (x * x) + a_turns * (z * z);
-    double sn, cs;
-    sincospi(2.0 * (t - rint(t)), &sn, &cs);
-    const double re = scale * (cr * cs - ci * sn);
-    const double im = scale * (cr * sn + ci * cs);
+    re *= scale;
+    im *= scale;
     if (first) {
         acc_re[idx] = re;
         acc_im[idx] = im;
@@ -608,18 +583,7 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     XK_CUDA_TRY(attr_err);
     int* d_err = ws.ctrl.as<int>();
     XK_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
-    // Per-ray factors, one record per ray of every block (padding included).
-    const size_t n_pad = (size_t)sh.ray_blocks * kFRays;
-    XK_TRY(ws.staged.ensure(n_pad * sizeof(StagedRay)));
-    const double dxs = (in.x_max - in.x_min) / (double)(nx > 1 ? nx - 1 : 1);
-    const double dzs = (in.z_max - in.z_min) / (double)(nz > 1 ? nz - 1 : 1);
-    fresnel_stage_kernel<<<grid_1d(n_pad, 256), 256, 0, stream>>>(
-        in.rx, in.rz, in.er, in.ei, n, n_pad, ox, oz, pre * kInv2Pi, dxs, dzs, 1.0 / in.max_amp,
-        ws.staged.as<StagedRay>());
-    XK_CUDA_TRY(cudaGetLastError());
-    rep->kernels += 1;
     FusedArgs fa;
-    fa.staged = ws.staged.as<StagedRay>();
     fa.rx = in.rx;
     fa.rz = in.rz;
     fa.er = in.er;
@@ -635,8 +599,6 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     fa.inv_scale = 1.0 / in.max_amp;
     fa.ox = ox;
     fa.oz = oz;
-    fa.dx = dxs;
-    fa.dz = dzs;
     fa.partial = ws.partial.as<double>();
     fa.m_pad = (int)sh.m_pad;
     fa.n_pad = (int)sh.n_pad;
@@ -648,9 +610,9 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     fresnel_fused_kernel<<<grid, kFThreads, kFSmem, stream>>>(fa);
     XK_CUDA_TRY(cudaGetLastError());
     if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[1], stream));
-    reduce_kernel<<<grid_1d(m, 256), 256, 0, stream>>>(
-        ws.partial.as<double>(), sh.splits, (int)sh.m_pad, (int)sh.n_pad, nz, nx, in.max_amp, xp,
-        zp, ox, oz, pre * kInv2Pi, in.out_re, in.out_im, 1);
+    reduce_kernel<<<grid_1d(m, 256), 256, 0, stream>>>(ws.partial.as<double>(), sh.splits,
+                                                        (int)sh.m_pad, (int)sh.n_pad, nz, nx,
+                                                        in.max_amp, in.out_re, in.out_im, 1);
     XK_CUDA_TRY(cudaGetLastError());
     rep->kernels += 2;
     if (timed) {

@@ -177,7 +177,6 @@ struct FresnelShape {
 
 struct FresnelWorkspace {
     DevBuf coords, partial, ctrl;
-    DevBuf staged;  // per-ray phase factors of the tensor-core product (48 B per ray)
     uint32_t wait_limit = 1u << 24;  // polls of every bounded wait of the tensor-core product
 };
 

@@ -62,6 +62,10 @@ constexpr int kFoldStages = 1;
 constexpr double kSeriesRcpBound = 2e-3;
 // Fold the base phase when the estimated chunks per ray group reach this.
 constexpr double kFoldChunksPerGroup = 4.0;
+// ... and chunks average fewer rays than this: a chunk switch (the points'
+// double-double base phase and the flush of the chunk sums) costs about as
+// much as sweeping 30 rays, the folded sweep about 8 % more per ray.
+constexpr double kFoldRaysPerChunk = 512.0;
 // Largest |es_j ep_0 - ep_j es_0| / (|es_j| |ep_0| + |ep_j| |es_0|) over the
 // rays under which every ray counts as having ray 0's polarization (2^-24:
 // the per-ray deviation is then below the FP32 rounding of the amplitudes
@@ -658,12 +662,12 @@ __device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int 
 
 // Prepares the stage's rays for the item direction (lane j handles rays
 // j, j+32).
-// One-polarization kernels (POL) prepare the one amplitude column they sum;
-// the unfolded ones (POLAR) keep it in polar form, e = {|a|, psi}, psi the
-// amplitude's phase plus the ray phase -k u.rho, which the sweep adds to the
-// pair's residual phase inside the FMA that forms it, so that a pair costs
-// one multiply and two FMAs on the sums instead of a complex multiply-add.
-template <bool POL, bool POLAR>
+// One-polarization kernels (POL) keep the one amplitude column they sum in
+// polar form, e = {|a|, psi}, psi the amplitude's phase plus the ray phase
+// -k u.rho, which the sweep adds to the pair's residual phase inside the FMA
+// that forms it, so that a pair costs one multiply and two FMAs on the sums
+// instead of a complex multiply-add.
+template <bool POL>
 __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, const PrSolve& sv,
                                            const WarpShared& ws) {
     const double ux = ws.ux, uy = ws.uy, uz = ws.uz;
@@ -675,20 +679,17 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
         double turns = -sv.kt * ur;
         float f = (float)(turns - rint(turns));
         float sn = 0.f, cs = 1.f;
-        if (!POLAR) __sincosf(6.28318530717958647692f * f, &sn, &cs);
+        if (!POL) __sincosf(6.28318530717958647692f * f, &sn, &cs);
         float rxf = (float)r.rx, ryf = (float)r.ry, rzf = (float)r.rz;
         float w = (float)(-2.0 * ur);
         float4 a = make_float4(rxf, ryf, rzf, (float)(sv.k * perp2));
         float4 b = make_float4(w, -2.f * (r.nx * rxf + r.ny * ryf + r.nz * rzf), r.nl, -w);
         float4 e;
-        if (POLAR) {
+        if (POL) {
             const float pr = sv.amp_src ? r.ep_re : r.es_re, pi = sv.amp_src ? r.ep_im : r.es_im;
             // |psi| <= 2 pi: f in [-1/2, 1/2] turns, atan2 in [-pi, pi].
             e = make_float4(hypotf(pr, pi), fmaf(6.28318530717958647692f, f, atan2f(pi, pr)),
                             0.f, 0.f);
-        } else if (POL) {
-            const float pr = sv.amp_src ? r.ep_re : r.es_re, pi = sv.amp_src ? r.ep_im : r.es_im;
-            e = make_float4(pr * cs - pi * sn, pr * sn + pi * cs, 0.f, 0.f);
         } else {
             e = make_float4(r.es_re * cs - r.es_im * sn, r.es_re * sn + r.es_im * cs,
                             r.ep_re * cs - r.ep_im * sn, r.ep_re * sn + r.ep_im * cs);
@@ -773,8 +774,11 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             num = fmaf(ls.vy[i], a.y, num);
             num = fmaf(ls.vz[i], a.z, num);
             const float rd = rcp_approx(ls.q2[i] + b.x);
-            constexpr bool POLAR = POL && !FOLD;
-            const float th = FOLD ? fmaf(num, rd, ls.phi[i]) : (POLAR ? fmaf(num, rd, e.y) : num * rd);
+            // One column: the amplitude's phase e.y joins the residual phase
+            // (folded: with the point's base phase, |phi + psi| <= 3 pi, so
+            // their sum rounds at ~2e-7 rad and th keeps one rounding).
+            const float th = POL ? fmaf(num, rd, FOLD ? ls.phi[i] + e.y : e.y)
+                                 : (FOLD ? fmaf(num, rd, ls.phi[i]) : num * rd);
             float sn, cs;
             __sincosf(th, &sn, &cs);
             float gq;
@@ -785,7 +789,7 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             }
             const float obl = fmaf(gq, rd, b.z);
             const float amp = obl * rd;
-            if (POLAR) {
+            if (POL) {
                 const float m = amp * e.x;
                 ls.acc[i][0] = fmaf(m, cs, ls.acc[i][0]);
                 ls.acc[i][1] = fmaf(m, sn, ls.acc[i][1]);
@@ -836,9 +840,8 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             const float2 ep = __fmul2_rn(wn, ls.q2[i]);
             const float2 rd = LIN ? __ffma2_rn(ls.q2[i], ep, ls.q2[i])
                                   : __ffma2_rn(ls.q2[i], __ffma2_rn(ep, ep, ep), ls.q2[i]);
-            constexpr bool POLAR = POL && !FOLD;
-            const float2 th = FOLD ? __ffma2_rn(num, rd, ls.phi[i])
-                                   : (POLAR ? __ffma2_rn(num, rd, ey) : __fmul2_rn(num, rd));
+            const float2 th = POL ? __ffma2_rn(num, rd, FOLD ? __fadd2_rn(ls.phi[i], ey) : ey)
+                                  : (FOLD ? __ffma2_rn(num, rd, ls.phi[i]) : __fmul2_rn(num, rd));
             float s0, c0, s1, c1;
             __sincosf(th.x, &s0, &c0);
             __sincosf(th.y, &s1, &c1);
@@ -851,7 +854,7 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             }
             const float2 obl = __ffma2_rn(gq, rd, nl);
             const float2 amp = __fmul2_rn(obl, rd);
-            if (POLAR) {
+            if (POL) {
                 const float2 m = __fmul2_rn(amp, ex);
                 ls.acc[i][0] = __ffma2_rn(m, f2(c0, c1), ls.acc[i][0]);
                 ls.acc[i][1] = __ffma2_rn(m, f2(s0, s1), ls.acc[i][1]);
@@ -977,7 +980,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
             setup_points<UNIFORM, FAST, FOLD>(sv, t, lane, ws, st);
             cur_chunk = c;
         }
-        prep_stage<POL, POL && !FOLD>(wp.buf[b], len, lane, sv, ws);
+        prep_stage<POL>(wp.buf[b], len, lane, sv, ws);
         __syncwarp();
         sweep_stage<UNIFORM, FOLD, POL, LIN>(wp.buf[b], len, lane, st, ws);
         // FP32 partials run over at most kFoldStages stages of one chunk.
@@ -1640,13 +1643,15 @@ Status pr_plan(const PrSolveIn* in, int count, PrWorkspace& ws, cudaStream_t str
                             P.rcp_bound * P.rcp_bound * budget <= 0.1 * o.tolerance));
         {
             // Fold the base phase into the sweep when ray groups span many
-            // chunks (near field): per-chunk flushes then disappear, at the
-            // price of a three-operand phase FMA per pair (about 1.4 % of the
-            // sweep). Non-empty cells bound the chunk count from above.
+            // chunks and chunks hold few rays (near field): per-chunk set-up
+            // and flushes then disappear, at the price of a phase add per
+            // pair in the sweep. Non-empty cells bound the chunk count from
+            // above.
             double cells = 1.0;
             for (int ax = 0; ax < 3; ++ax) cells *= (double)cg.n[ax];
             const double est_chunks = std::min(cells, (double)n);
-            P.fold = est_chunks >= kFoldChunksPerGroup * (double)groups[s];
+            P.fold = est_chunks >= kFoldChunksPerGroup * (double)groups[s] &&
+                     (double)n < kFoldRaysPerChunk * est_chunks;
         }
 
         ray_keys_kernel<<<(n + 255) / 256, 256, 0, stream>>>(in[s].rays, n, cg, B.rk_in, B.ri_in);
