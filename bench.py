@@ -910,17 +910,16 @@ def main():
     one_col = bool(stats["one_polarization"])
     # The sweep as issued, per ray x screen pair: FMA-pipe lane cycles (an
     # f32x2 instruction holds the pipe for two lanes' worth) and MUFU results.
-    # One amplitude column is carried in polar form: the sums take one f32x2
-    # multiply and two FMAs per pair of points instead of two multiplies and
-    # four FMAs; the folded (near-field) kernels add the point's base phase to
-    # the amplitude's phase, one add more.
-    fold = 1 if stats["folded"] else 0
+    # One amplitude column in the unfolded kernels is carried in polar form:
+    # the sums take one f32x2 multiply and two FMAs per pair of points instead
+    # of two multiplies and four FMAs (3 lane cycles fewer per pair).
+    polar = one_col and not stats["folded"]
     if stats["sweep"] == 1:
-        cyc, mufu = (14 + fold) if one_col else 21, 2
+        cyc, mufu = (14 if polar else 17) if one_col else 21, 2
     elif stats["sweep"] == 2:  # one f32x2 FMA fewer per pair of points
-        cyc, mufu = (13 + fold) if one_col else 20, 2
+        cyc, mufu = (13 if polar else 16) if one_col else 20, 2
     else:
-        cyc, mufu = (12 + fold) if one_col else 20, 3
+        cyc, mufu = (12 if polar else 16) if one_col else 20, 3
     ceiling = sms * min(fma_rate / cyc, mufu_rate / mufu) * clk_mhz * 1e6 / 1e9
     kms = float(np.mean(kern_ms))
     achieved = pairs / (kms / 1e3) / 1e9

@@ -65,15 +65,19 @@ def test_one_polarization_matches_two_columns_and_oracle(pol_ctx, oracle, name):
     two, st2 = run(pol_ctx, rays, pix)
     assert st2["one_polarization"] == 0
     if name != "es_zero":
-        # The summed column is es. The one-column far-field kernel carries it
-        # in polar form (its phase joins the pair's residual phase), so Es
-        # agrees with the two-column kernel's to FP32 rounding, not bitwise.
+        # The summed column is es. The folded one-column kernel sums it with
+        # the FP32 operations of the two-column kernel's Es sum: bit for bit
+        # the same Es. The unfolded one carries it in polar form (its phase
+        # joins the pair's residual phase): another rounding of the same sum.
         es1 = one[0] + 1j * one[1]
         es2 = two[0] + 1j * two[1]
-        assert np.linalg.norm(es1 - es2) / np.linalg.norm(es2) < 1e-6
+        if st1["folded"]:
+            assert np.array_equal(one[0], two[0]) and np.array_equal(one[1], two[1])
+        else:
+            assert np.linalg.norm(es1 - es2) / np.linalg.norm(es2) < 5e-5
     ref = oracle.kahan_f64(*cases.as_lists(rays, pix))
     assert cases.rel_l2(one, ref) < PR_TOL
-    assert cases.rel_l2(one, two) < 1e-6
+    assert cases.rel_l2(one, two) < (1e-6 if st1["folded"] else 5e-5)
     if name == "reference_bench":
         assert not np.any(one[2]) and not np.any(one[3])
     if name == "es_zero":
@@ -111,3 +115,21 @@ def test_config1_workload_is_one_polarization(ctx):
     rays, screen = synth.config1(seed=0, n_rays=1 << 14, grid=64)
     _, st = run(ctx, rays, screen)
     assert st["one_polarization"] == 1
+
+
+def test_unfolded_polar_one_column_matches_two_columns(pol_ctx, oracle):
+    """The far-field one-column kernel (unfolded, amplitude in polar form) on
+    the 10 keV, 1 m aperture: within the tolerance of the extended-precision
+    oracle, and within FP32-PR noise of the two-column kernel."""
+    rays, screen = synth.config1(seed=4, n_rays=1 << 18, grid=256)
+    one, st1 = run(pol_ctx, rays, screen)
+    assert st1["one_polarization"] == 1 and st1["folded"] == 0
+    pol_ctx.set_option("polarization", 0)
+    two, st2 = run(pol_ctx, rays, screen)
+    assert st2["one_polarization"] == 0
+    assert cases.rel_l2(one, two) < 5e-5
+    sub, idx = synth.subsample_screen(screen, 128, seed=2)
+    exact = oracle.kahan_ld(*cases.as_lists(rays, sub))
+    got = [o[idx] for o in one]
+    assert cases.rel_l2(got, exact) < PR_TOL
+    assert cases.rel_l2_intensity(got, exact) < PR_TOL

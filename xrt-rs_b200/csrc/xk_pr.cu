@@ -662,12 +662,14 @@ __device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int 
 
 // Prepares the stage's rays for the item direction (lane j handles rays
 // j, j+32).
-// One-polarization kernels (POL) keep the one amplitude column they sum in
-// polar form, e = {|a|, psi}, psi the amplitude's phase plus the ray phase
-// -k u.rho, which the sweep adds to the pair's residual phase inside the FMA
-// that forms it, so that a pair costs one multiply and two FMAs on the sums
-// instead of a complex multiply-add.
-template <bool POL>
+// One-polarization kernels (POL) prepare the one amplitude column they sum;
+// the unfolded ones (POLAR) keep it in polar form, e = {|a|, psi}, psi the
+// amplitude's phase plus the ray phase -k u.rho, which the sweep adds to the
+// pair's residual phase inside the FMA that forms it, so that a pair costs
+// one multiply and two FMAs on the sums instead of a complex multiply-add.
+// (In the folded kernels the same form measured 3x the field error and no
+// faster; they keep the Cartesian amplitude.)
+template <bool POL, bool POLAR>
 __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, const PrSolve& sv,
                                            const WarpShared& ws) {
     const double ux = ws.ux, uy = ws.uy, uz = ws.uz;
@@ -679,17 +681,20 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
         double turns = -sv.kt * ur;
         float f = (float)(turns - rint(turns));
         float sn = 0.f, cs = 1.f;
-        if (!POL) __sincosf(6.28318530717958647692f * f, &sn, &cs);
+        if (!POLAR) __sincosf(6.28318530717958647692f * f, &sn, &cs);
         float rxf = (float)r.rx, ryf = (float)r.ry, rzf = (float)r.rz;
         float w = (float)(-2.0 * ur);
         float4 a = make_float4(rxf, ryf, rzf, (float)(sv.k * perp2));
         float4 b = make_float4(w, -2.f * (r.nx * rxf + r.ny * ryf + r.nz * rzf), r.nl, -w);
         float4 e;
-        if (POL) {
+        if (POLAR) {
             const float pr = sv.amp_src ? r.ep_re : r.es_re, pi = sv.amp_src ? r.ep_im : r.es_im;
             // |psi| <= 2 pi: f in [-1/2, 1/2] turns, atan2 in [-pi, pi].
             e = make_float4(hypotf(pr, pi), fmaf(6.28318530717958647692f, f, atan2f(pi, pr)),
                             0.f, 0.f);
+        } else if (POL) {
+            const float pr = sv.amp_src ? r.ep_re : r.es_re, pi = sv.amp_src ? r.ep_im : r.es_im;
+            e = make_float4(pr * cs - pi * sn, pr * sn + pi * cs, 0.f, 0.f);
         } else {
             e = make_float4(r.es_re * cs - r.es_im * sn, r.es_re * sn + r.es_im * cs,
                             r.ep_re * cs - r.ep_im * sn, r.ep_re * sn + r.ep_im * cs);
@@ -774,11 +779,10 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             num = fmaf(ls.vy[i], a.y, num);
             num = fmaf(ls.vz[i], a.z, num);
             const float rd = rcp_approx(ls.q2[i] + b.x);
-            // One column: the amplitude's phase e.y joins the residual phase
-            // (folded: with the point's base phase, |phi + psi| <= 3 pi, so
-            // their sum rounds at ~2e-7 rad and th keeps one rounding).
-            const float th = POL ? fmaf(num, rd, FOLD ? ls.phi[i] + e.y : e.y)
-                                 : (FOLD ? fmaf(num, rd, ls.phi[i]) : num * rd);
+            // One column, unfolded: the amplitude's phase e.y joins the
+            // residual phase inside the FMA that forms it.
+            constexpr bool POLAR = POL && !FOLD;
+            const float th = FOLD ? fmaf(num, rd, ls.phi[i]) : (POLAR ? fmaf(num, rd, e.y) : num * rd);
             float sn, cs;
             __sincosf(th, &sn, &cs);
             float gq;
@@ -789,7 +793,7 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             }
             const float obl = fmaf(gq, rd, b.z);
             const float amp = obl * rd;
-            if (POL) {
+            if (POLAR) {
                 const float m = amp * e.x;
                 ls.acc[i][0] = fmaf(m, cs, ls.acc[i][0]);
                 ls.acc[i][1] = fmaf(m, sn, ls.acc[i][1]);
@@ -840,8 +844,9 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             const float2 ep = __fmul2_rn(wn, ls.q2[i]);
             const float2 rd = LIN ? __ffma2_rn(ls.q2[i], ep, ls.q2[i])
                                   : __ffma2_rn(ls.q2[i], __ffma2_rn(ep, ep, ep), ls.q2[i]);
-            const float2 th = POL ? __ffma2_rn(num, rd, FOLD ? __fadd2_rn(ls.phi[i], ey) : ey)
-                                  : (FOLD ? __ffma2_rn(num, rd, ls.phi[i]) : __fmul2_rn(num, rd));
+            constexpr bool POLAR = POL && !FOLD;
+            const float2 th = FOLD ? __ffma2_rn(num, rd, ls.phi[i])
+                                   : (POLAR ? __ffma2_rn(num, rd, ey) : __fmul2_rn(num, rd));
             float s0, c0, s1, c1;
             __sincosf(th.x, &s0, &c0);
             __sincosf(th.y, &s1, &c1);
@@ -854,7 +859,7 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
             }
             const float2 obl = __ffma2_rn(gq, rd, nl);
             const float2 amp = __fmul2_rn(obl, rd);
-            if (POL) {
+            if (POLAR) {
                 const float2 m = __fmul2_rn(amp, ex);
                 ls.acc[i][0] = __ffma2_rn(m, f2(c0, c1), ls.acc[i][0]);
                 ls.acc[i][1] = __ffma2_rn(m, f2(s0, s1), ls.acc[i][1]);
@@ -980,7 +985,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
             setup_points<UNIFORM, FAST, FOLD>(sv, t, lane, ws, st);
             cur_chunk = c;
         }
-        prep_stage<POL>(wp.buf[b], len, lane, sv, ws);
+        prep_stage<POL, POL && !FOLD>(wp.buf[b], len, lane, sv, ws);
         __syncwarp();
         sweep_stage<UNIFORM, FOLD, POL, LIN>(wp.buf[b], len, lane, st, ws);
         // FP32 partials run over at most kFoldStages stages of one chunk.
