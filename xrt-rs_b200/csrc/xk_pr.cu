@@ -26,7 +26,7 @@
 // for every (tile, cell) pair; each occupied cell is a chunk. The sorted ray
 // list is cut into `groups` equal ranges; an item is (tile, range), and the
 // persistent kernel's warps claim items from an atomic counter. Inside an
-// item the range is streamed through shared memory 64 rays at a time by
+// item the range is streamed through shared memory kPrStage rays at a time by
 // cp.async.bulk (TMA bulk copy, mbarrier completion, two buffers), prepared
 // in place for the item's direction u, and swept by all 32 lanes. Each lane
 // keeps per-point FP32 partial sums folded every stage into two-float
@@ -489,14 +489,18 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 //   e = {es', ep'} with the per-ray phasor exp(-i k u.rho) applied
 //   n = {2 nx, 2 ny, 2 nz, 0}
 //
-// Per-warp shared state besides the two ray buffers.
-struct WarpShared {
-    float hi[kPrPpl * 4][32];  // two-float accumulators, [point*4 + component][lane]
-    float lo[kPrPpl * 4][32];
-    float2 ph[kPrPpl][32];     // (k/2pi) i exp(i k |q|) of the current chunk (unfolded variants)
-    double ux, uy, uz;         // item direction for the current chunk
-    double r0x, r0y, r0z;      // chunk centre
-    uint64_t bar[2];           // mbarriers of the two ray buffers
+// Per-warp shared state besides the two ray buffers. NC components per point:
+// 4 (Es, Ep) or 2 (the one-polarization kernels' single column), which is
+// what lets those kernels fit four CTAs per SM.
+template <int NC>
+struct WarpSharedT {
+    static constexpr int kNC = NC;
+    float hi[kPrPpl * NC][32];  // two-float accumulators, [point*NC + component][lane]
+    float lo[kPrPpl * NC][32];
+    float2 ph[kPrPpl][32];      // (k/2pi) i exp(i k |q|) of the current chunk (unfolded variants)
+    double ux, uy, uz;          // item direction for the current chunk
+    double r0x, r0y, r0z;       // chunk centre
+    uint64_t bar[2];            // mbarriers of the two ray buffers
 };
 
 // Per-lane state of the SFU sweep.
@@ -553,8 +557,8 @@ __device__ __forceinline__ double dd_turns(double kt_hi, double kt_lo, double qx
 // Per chunk: FP64 geometry of the lane's points, written into the sweep
 // state, and the per-point base phase k|q|: folded into the sweep state
 // (FOLD) or as the chunk phasor (k/2pi) i exp(i k|q|) into shared memory.
-template <bool UNIFORM, bool FAST, bool FOLD, class State>
-__device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane, WarpShared& ws,
+template <bool UNIFORM, bool FAST, bool FOLD, class State, class WS>
+__device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane, WS& ws,
                                              State& st) {
     const double ux = ws.ux, uy = ws.uy, uz = ws.uz;
     const double r0x = ws.r0x, r0y = ws.r0y, r0z = ws.r0z;
@@ -605,9 +609,9 @@ __device__ __forceinline__ void setup_points(const PrSolve& sv, int t, int lane,
 // Unfolded variants, at every chunk boundary and at the item end: multiplies
 // the lane's two-float chunk sums by the chunk phasor in FP64, adds them to
 // the item's slots (tile-slot order) and clears the sums.
-template <bool POL>
-__device__ __forceinline__ void flush_chunk(const PrSolve& sv, int t, int g, int lane,
-                                            WarpShared& ws) {
+template <bool POL, class WS>
+__device__ __forceinline__ void flush_chunk(const PrSolve& sv, int t, int g, int lane, WS& ws) {
+    constexpr int NC = WS::kNC;
     const size_t slots = (size_t)sv.n_tiles * kPrTile;
     double* base = sv.partial + (size_t)g * 4 * slots;
 #pragma unroll 2
@@ -618,9 +622,9 @@ __device__ __forceinline__ void flush_chunk(const PrSolve& sv, int t, int g, int
         double v[4];
 #pragma unroll
         for (int c = 0; c < (POL ? 2 : 4); ++c) {
-            v[c] = (double)ws.hi[i * 4 + c][lane] + (double)ws.lo[i * 4 + c][lane];
-            ws.hi[i * 4 + c][lane] = 0.f;
-            ws.lo[i * 4 + c][lane] = 0.f;
+            v[c] = (double)ws.hi[i * NC + c][lane] + (double)ws.lo[i * NC + c][lane];
+            ws.hi[i * NC + c][lane] = 0.f;
+            ws.lo[i * NC + c][lane] = 0.f;
         }
         // Each slot is updated by this one thread, in chunk order; the atomic
         // form only lets the warp go on without waiting for the loads.
@@ -635,9 +639,9 @@ __device__ __forceinline__ void flush_chunk(const PrSolve& sv, int t, int g, int
 
 // Folded variants, once at the item end: multiplies the lane's two-float
 // sums of the item by i k / (2 pi) in FP64 and adds them to the item's slots.
-template <bool POL>
-__device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int lane,
-                                             WarpShared& ws) {
+template <bool POL, class WS>
+__device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int lane, WS& ws) {
+    constexpr int NC = WS::kNC;
     const size_t slots = (size_t)sv.n_tiles * kPrTile;
     double* base = sv.partial + (size_t)g * 4 * slots;
     const double kt = sv.kt;
@@ -647,7 +651,7 @@ __device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int 
         double v[4];
 #pragma unroll
         for (int c = 0; c < (POL ? 2 : 4); ++c)
-            v[c] = (double)ws.hi[i * 4 + c][lane] + (double)ws.lo[i * 4 + c][lane];
+            v[c] = (double)ws.hi[i * NC + c][lane] + (double)ws.lo[i * NC + c][lane];
         // Sub-items of one (group, tile) add into the same slots in sub
         // order (never two in one launch); the atomic form only lets the warp
         // go on without waiting for the loads.
@@ -669,9 +673,9 @@ __device__ __forceinline__ void flush_item(const PrSolve& sv, int t, int g, int 
 // one multiply and two FMAs on the sums instead of a complex multiply-add.
 // (In the folded kernels the same form measured 3x the field error and no
 // faster; they keep the Cartesian amplitude.)
-template <bool POL, bool POLAR>
+template <bool POL, bool POLAR, class WS>
 __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, const PrSolve& sv,
-                                           const WarpShared& ws) {
+                                           const WS& ws) {
     const double ux = ws.ux, uy = ws.uy, uz = ws.uz;
     for (int j = lane; j < len; j += 32) {
         const PrRawRay r = buf[j];
@@ -711,35 +715,37 @@ __device__ __forceinline__ void prep_stage(PrRawRay* buf, int len, int lane, con
 // Adds the lane's FP32 partials into its two-float accumulators and clears
 // them (every kFoldStages stages and at chunk and item ends).
 // One-polarization kernels (POL) carry components 0 and 1 only.
-template <bool POL, bool UNIFORM>
-__device__ __forceinline__ void fold_acc(ScalarState<UNIFORM>& ls, WarpShared& ws, int lane) {
+template <bool POL, bool UNIFORM, class WS>
+__device__ __forceinline__ void fold_acc(ScalarState<UNIFORM>& ls, WS& ws, int lane) {
+    constexpr int NC = WS::kNC;
 #pragma unroll
     for (int i = 0; i < kPrPpl; ++i)
 #pragma unroll
         for (int c = 0; c < (POL ? 2 : 4); ++c) {
-            float hi = ws.hi[i * 4 + c][lane], lo = ws.lo[i * 4 + c][lane];
+            float hi = ws.hi[i * NC + c][lane], lo = ws.lo[i * NC + c][lane];
             two_sum_acc(hi, lo, ls.acc[i][c]);
-            ws.hi[i * 4 + c][lane] = hi;
-            ws.lo[i * 4 + c][lane] = lo;
+            ws.hi[i * NC + c][lane] = hi;
+            ws.lo[i * NC + c][lane] = lo;
             ls.acc[i][c] = 0.f;
         }
 }
 
-template <bool POL, bool UNIFORM>
-__device__ __forceinline__ void fold_acc(PackedState<UNIFORM>& ls, WarpShared& ws, int lane) {
+template <bool POL, bool UNIFORM, class WS>
+__device__ __forceinline__ void fold_acc(PackedState<UNIFORM>& ls, WS& ws, int lane) {
+    constexpr int NC = WS::kNC;
 #pragma unroll
     for (int i = 0; i < kPrPpl / 2; ++i)
 #pragma unroll
         for (int c = 0; c < (POL ? 2 : 4); ++c) {
             const float2 v = ls.acc[i][c];
-            float hi0 = ws.hi[(2 * i) * 4 + c][lane], lo0 = ws.lo[(2 * i) * 4 + c][lane];
-            float hi1 = ws.hi[(2 * i + 1) * 4 + c][lane], lo1 = ws.lo[(2 * i + 1) * 4 + c][lane];
+            float hi0 = ws.hi[(2 * i) * NC + c][lane], lo0 = ws.lo[(2 * i) * NC + c][lane];
+            float hi1 = ws.hi[(2 * i + 1) * NC + c][lane], lo1 = ws.lo[(2 * i + 1) * NC + c][lane];
             two_sum_acc(hi0, lo0, v.x);
             two_sum_acc(hi1, lo1, v.y);
-            ws.hi[(2 * i) * 4 + c][lane] = hi0;
-            ws.lo[(2 * i) * 4 + c][lane] = lo0;
-            ws.hi[(2 * i + 1) * 4 + c][lane] = hi1;
-            ws.lo[(2 * i + 1) * 4 + c][lane] = lo1;
+            ws.hi[(2 * i) * NC + c][lane] = hi0;
+            ws.lo[(2 * i) * NC + c][lane] = lo0;
+            ws.hi[(2 * i + 1) * NC + c][lane] = hi1;
+            ws.lo[(2 * i + 1) * NC + c][lane] = lo1;
             ls.acc[i][c] = f2(0.f);
         }
 }
@@ -762,9 +768,9 @@ __device__ __forceinline__ void clear_acc(PackedState<UNIFORM>& ls) {
 
 // SFU sweep: one point per FP32 instruction, rcp.approx for the reciprocal
 // (LIN does not apply).
-template <bool UNIFORM, bool FOLD, bool POL, bool LIN>
+template <bool UNIFORM, bool FOLD, bool POL, bool LIN, class WS>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
-                                            ScalarState<UNIFORM>& ls, WarpShared& ws) {
+                                            ScalarState<UNIFORM>& ls, WS& ws) {
     const float4* rec = reinterpret_cast<const float4*>(buf);
 #pragma unroll 1
     for (int j = 0; j < len; ++j) {
@@ -814,9 +820,9 @@ __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int la
 // r0 (1 + e + e^2), or r0 (1 + e) when the planner bounds |e|^2 times the
 // phase budget far below the tolerance (LIN: one f32x2 FMA fewer per pair of
 // points).
-template <bool UNIFORM, bool FOLD, bool POL, bool LIN>
+template <bool UNIFORM, bool FOLD, bool POL, bool LIN, class WS>
 __device__ __forceinline__ void sweep_stage(const PrRawRay* buf, int len, int lane,
-                                            PackedState<UNIFORM>& ls, WarpShared& ws) {
+                                            PackedState<UNIFORM>& ls, WS& ws) {
     constexpr int H = kPrPpl / 2;
     const float4* rec = reinterpret_cast<const float4*>(buf);
     // Two rays per iteration give the scheduler two independent sets of
@@ -906,7 +912,8 @@ __device__ __forceinline__ int chunk_of(const int* __restrict__ begin, int n_chu
 
 // Processes one (tile, ray-range) item; false if a bounded wait ran out.
 template <bool UNIFORM, bool FAST, bool FOLD, bool POL, bool LIN>
-__device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, WarpShared& ws,
+__device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp,
+                             WarpSharedT<POL ? 2 : 4>& ws,
                              int lane, uint32_t wait_limit, uint32_t stall_bytes) {
     // local = (sub * groups + g) * n_tiles + t: sub-range `sub` of ray group g
     // against tile t. Sub-items of one (g, t) add into the same slots, so a
@@ -926,7 +933,7 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
     const int* __restrict__ cb = sv.chunk_begin;
 
 #pragma unroll
-    for (int i = 0; i < kPrPpl * 4; ++i) ws.hi[i][lane] = ws.lo[i][lane] = 0.f;
+    for (int i = 0; i < kPrPpl * (POL ? 2 : 4); ++i) ws.hi[i][lane] = ws.lo[i][lane] = 0.f;
 
     using State = typename std::conditional<FAST, PackedState<UNIFORM>, ScalarState<UNIFORM>>::type;
     State st;
@@ -1014,14 +1021,14 @@ __device__ bool process_item(const PrSolve& sv, long long local, WarpPipe& wp, W
 // launch, and the launch covers items [item_offset, item_offset + count) of
 // each solve.
 template <bool UNIFORM, bool FAST, bool FOLD, bool POL, bool LIN>
-__global__ void __launch_bounds__(kPrWarpsPerCta * 32, 3)
+__global__ void __launch_bounds__(kPrWarpsPerCta * 32, (POL && !FOLD) ? 4 : 3)
 pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long n_items,
                      unsigned long long* __restrict__ counter, int* __restrict__ err, PrCtl ctl) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     PrRawRay* bufs = reinterpret_cast<PrRawRay*>(smem) + warp * 2 * kPrStage;
-    WarpShared* wsh = reinterpret_cast<WarpShared*>(
-                          smem + kPrWarpsPerCta * 2 * kPrStage * sizeof(PrRawRay)) + warp;
+    using WS = WarpSharedT<POL ? 2 : 4>;
+    WS* wsh = reinterpret_cast<WS*>(smem + kPrWarpsPerCta * 2 * kPrStage * sizeof(PrRawRay)) + warp;
     WarpPipe wp;
     wp.buf[0] = bufs;
     wp.buf[1] = bufs + kPrStage;
@@ -1057,8 +1064,11 @@ pr_persistent_kernel(const PrSolve* __restrict__ solves, int n_solves, long long
     }
 }
 
-constexpr size_t kPrSmemBytes = (size_t)kPrWarpsPerCta * 2 * kPrStage * sizeof(PrRawRay) +
-                                (size_t)kPrWarpsPerCta * sizeof(WarpShared);
+// Dynamic shared memory of a launch: the warps' ray buffers and their state.
+constexpr size_t pr_smem_bytes(bool pol) {
+    return (size_t)kPrWarpsPerCta * 2 * kPrStage * sizeof(PrRawRay) +
+           (size_t)kPrWarpsPerCta * (pol ? sizeof(WarpSharedT<2>) : sizeof(WarpSharedT<4>));
+}
 
 using PrKernel = void (*)(const PrSolve*, int, long long, unsigned long long*, int*, PrCtl);
 
@@ -1731,17 +1741,17 @@ Status pr_launch(const PrSolve* d_table, int n_solves, long long n_items, int va
                  int max_ctas_per_sm, const PrCtl& ctl) {
     if (n_items <= 0) return Status::Ok();
     PrKernel kern = pr_kernel(variant);
-    XK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kPrSmemBytes));
+    const size_t smem = pr_smem_bytes((variant & 8) != 0);
+    XK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     XK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPrWarpsPerCta * 32,
-                                                              kPrSmemBytes));
+                                                              smem));
     per_sm = std::max(per_sm, 1);
     if (max_ctas_per_sm > 0) per_sm = std::min(per_sm, max_ctas_per_sm);
     long long grid = (long long)num_sms * per_sm;
     grid = std::max<long long>(1, std::min(grid, (n_items + kPrWarpsPerCta - 1) / kPrWarpsPerCta));
-    kern<<<(unsigned)grid, kPrWarpsPerCta * 32, kPrSmemBytes, stream>>>(d_table, n_solves, n_items,
-                                                                        d_counter, d_err, ctl);
+    kern<<<(unsigned)grid, kPrWarpsPerCta * 32, smem, stream>>>(d_table, n_solves, n_items,
+                                                                d_counter, d_err, ctl);
     XK_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
 }

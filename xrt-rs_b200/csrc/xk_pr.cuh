@@ -11,7 +11,7 @@ namespace xk {
 
 // Geometry of the work decomposition.
 constexpr int kPrWarpsPerCta = 4;
-constexpr int kPrStage = 64;          // rays per shared-memory stage
+constexpr int kPrStage = 56;          // rays per shared-memory stage
 constexpr int kPrPpl = 8;             // screen points per lane
 constexpr int kPrTile = 32 * kPrPpl;  // screen points per tile (one warp)
 
