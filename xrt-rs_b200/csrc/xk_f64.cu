@@ -117,8 +117,11 @@ __device__ __forceinline__ void pair_f64(const RayRec64& r, double px, double py
     kahan_add(a.s[3], a.c[3], ti);
 }
 
+// The kernel is issue-bound (about 400 instructions per pair with the library
+// sincos); capping registers at 80 for six CTAs per SM (24 warps instead of
+// 20) hides a little more latency: +4 % plain, +2 % reduced, same results.
 template <bool REDUCE>
-__global__ void __launch_bounds__(kF64Threads)
+__global__ void __launch_bounds__(kF64Threads, 6)
 f64_pairs_kernel(const RayRec64* __restrict__ rays, size_t n_rays, size_t rays_per_split,
                  PixDev pix, size_t n_pix, FieldDev out, double* __restrict__ partials) {
     __shared__ RayRec64 sm[kF64Stage];
