@@ -16,15 +16,18 @@
 //       exp(i a r^2) = exp(i a (x_ix - x_j)^2) * exp(i a (z_iz - z_j)^2),
 //   so U = Z diag(es) X^T is a complex matrix product with the ray index as
 //   the contraction. As a real product with interleaved (re, im) columns,
-//       C[iz][2 ix + c] = sum_k A[iz][k] B[2 ix + c][k],
+//       C[iz][n(ix, c)] = sum_k A[iz][k] B[n(ix, c)][k],
 //       A[iz][2j] = Re Z, A[iz][2j+1] = Im Z,
-//       B[2ix][2j] = Re W, B[2ix][2j+1] = -Im W, B[2ix+1][2j] = Im W, B[2ix+1][2j+1] = Re W,
-//   with W = es X / max|es|. One fused kernel computes it on the tensor
-//   cores without ever writing A or B to memory: per block of 32 rays, eight
-//   producer warps form the CTA's A (128 z rows) and B (128 x points, 256
-//   rows) tiles from FP64 phases, split each phasor into f16 hi + lo parts
-//   and store them in shared memory in the 128-byte-swizzled K-major layout;
-//   one thread issues tcgen05.mma kind::f16 (f32 accumulation in tensor
+//       B[n(ix,0)][2j] = Re W, B[n(ix,0)][2j+1] = -Im W, B[n(ix,1)][2j] = Im W, B[n(ix,1)][2j+1] = Re W,
+//   with W = es X / max|es| and, per 128-point block of x, the real parts in
+//   its first 128 columns and the imaginary parts in the next 128:
+//   n(ix, c) = 256 (ix / 128) + 128 c + ix % 128. One fused kernel computes
+//   it on the tensor cores without ever writing A or B to memory: per block
+//   of 32 rays, a stager warp writes the rays' split coordinates to a ring of
+//   shared-memory buffers, eight producer warps form the CTA's A (128 z rows)
+//   and B (128 x points, 256 rows) tiles from them, split each phasor into
+//   f16 hi + lo parts and store them in shared memory in the
+//   128-byte-swizzled K-major layout; one thread issues tcgen05.mma kind::f16 (f32 accumulation in tensor
 //   memory) for A_hi B_hi + A_hi B_lo + A_lo B_hi, which keeps ~2^-21 of each
 //   phasor; four epilogue warps drain the accumulator into an FP64 partial
 //   every kFSeg ray blocks (the tensor cores' f32 accumulation error grows
@@ -112,8 +115,20 @@ constexpr uint32_t kFA = 128 * 64 * 2;           // one A tile (hi or lo): 128 r
 constexpr uint32_t kFB = 256 * 64 * 2;           // one B tile: 256 rows x 128 B
 constexpr uint32_t kFStage = 2 * kFA + 2 * kFB;  // A_hi | A_lo | B_hi | B_lo
 constexpr int kFEpiThreads = 128;                // warps 1..4
-constexpr int kFProdThreads = 256;               // warps 5..12
-constexpr int kFThreads = 32 + kFEpiThreads + kFProdThreads;
+#ifndef XK_FRESNEL_PROD_WARPS
+#define XK_FRESNEL_PROD_WARPS 8
+#endif
+#ifndef XK_FRESNEL_ROWS_PER
+#define XK_FRESNEL_ROWS_PER 2
+#endif
+constexpr int kFProdThreads = 32 * XK_FRESNEL_PROD_WARPS;  // warps 5..
+constexpr int kFRowsPer = XK_FRESNEL_ROWS_PER;             // A rows (and x points) per producer
+constexpr int kFRowThreads = 128 / kFRowsPer;              // producers per ray group
+constexpr int kFChunks = 8 / (kFProdThreads / kFRowThreads);  // 16-byte chunks per producer
+static_assert(kFChunks * (kFProdThreads / kFRowThreads) == 8 && kFRowThreads % 32 == 0,
+              "producers must tile the 128 rows x 8 chunks of a block");
+constexpr int kFThreads = 32 + kFEpiThreads + kFProdThreads + 32;  // + the ray stager warp
+constexpr int kFRayBufs = 4;  // staged ray blocks in flight
 constexpr int kFSeg = 20;                        // ray blocks (60 K blocks) per f32 segment
 constexpr int kFN = 256;                         // accumulator columns (N of the UMMA)
 // Ray staging (two blocks), per ray 8 floats: x hi, x lo, frac(a x^2), z hi,
@@ -122,7 +137,7 @@ constexpr int kFN = 256;                         // accumulator columns (N of th
 constexpr uint32_t kFRayBytes = kFRays * 32;
 // Epilogue transpose buffers: per epilogue warp 32 x 33 floats.
 constexpr uint32_t kFEpiBytes = 4 * 32 * 33 * 4;
-constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + 2 * kFRayBytes + kFEpiBytes + 256;
+constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + kFRayBufs * kFRayBytes + kFEpiBytes + 256;
 
 struct FusedArgs {
     const double *rx, *rz, *er, *ei;
@@ -199,10 +214,6 @@ __device__ __forceinline__ void split16x2(float a, float b, uint32_t* hi, uint32
 __device__ __forceinline__ uint32_t neg_hi(uint32_t v) { return v ^ 0x80000000u; }
 __device__ __forceinline__ uint32_t swap_halves(uint32_t v) { return __byte_perm(v, 0, 0x1032); }
 
-__device__ __forceinline__ void producer_sync() {
-    asm volatile("bar.sync 1, %0;" ::"n"(kFProdThreads) : "memory");
-}
-
 __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g) {
     using namespace sm100;
     extern __shared__ unsigned char smem_raw[];
@@ -212,7 +223,9 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
     uint64_t* empty = full + kFStages;
     uint64_t* acc_full = empty + kFStages;
     uint64_t* acc_empty = acc_full + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+    uint64_t* ray_full = acc_empty + 2;
+    uint64_t* ray_empty = ray_full + kFRayBufs;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ray_empty + kFRayBufs);
     volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     unsigned char* rays_smem = reinterpret_cast<unsigned char*>(tmem_slot) + 64;
 
@@ -231,6 +244,10 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
             mbar_init(&acc_empty[b], kFEpiThreads);
+        }
+        for (int b = 0; b < kFRayBufs; ++b) {
+            mbar_init(&ray_full[b], 1);                      // the stager warp
+            mbar_init(&ray_empty[b], kFProdThreads / 32);  // one arrival per producer warp
         }
         mbar_init_fence();
         *flag = 0;
@@ -286,7 +303,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
         // transposed through shared memory so that the FP64 partial is
         // updated one row at a time, 32 consecutive columns per access.
         const int qd = warp & 3;
-        float* tb = reinterpret_cast<float*>(rays_smem + 2 * kFRayBytes) + (warp - 1) * 32 * 33;
+        float* tb = reinterpret_cast<float*>(rays_smem + kFRayBufs * kFRayBytes) + (warp - 1) * 32 * 33;
         double* rows0 = g.partial + ((size_t)sp * g.m_pad + (size_t)mt * 128 + qd * 32) * g.n_pad +
                         (size_t)nt * kFN + lane;
         if (nseg == 0)
@@ -325,122 +342,134 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             tc_fence_before();
             mbar_arrive(&acc_empty[b]);
         }
-    } else {
-        // Producers: thread p owns A row r (screen z index mt*128 + r) and B
-        // rows 2r, 2r+1 (screen x index nt*128 + r) for rays 16h .. 16h+15 of
-        // each block (h = p / 128), i.e. 16-byte chunks 4h .. 4h+3 of its rows.
-        // The block's rays are staged in shared memory one block ahead by
-        // threads 0..95 (rx, rz, scaled amplitude).
+    } else if (warp < 5 + kFProdThreads / 32) {
+        // Producers: thread p owns kFRowsPer A rows r_k = (p % kFRowThreads) +
+        // kFRowThreads k (screen z index mt*128 + r_k) and the B rows r_k,
+        // 128 + r_k (screen x index nt*128 + r_k), for the 16-byte chunks
+        // kFChunks q .. kFChunks (q + 1) - 1 (q = p / kFRowThreads) of each
+        // ray block: every staged ray value a thread reads serves kFRowsPer
+        // rows, and each store instruction of a warp covers 32 consecutive
+        // rows. The stager warp stages each block's rays in shared memory up
+        // to kFRayBufs blocks ahead.
         const int p = threadIdx.x - 160;
-        const int h = p >> 7, r = p & 127;
-        const size_t iz = (size_t)mt * 128 + r, ix = (size_t)nt * 128 + r;
-        const bool va = iz < g.nz, vb = ix < g.nx;
-        // Per-row terms: kappa = -2 a p (hi, lo) and P = frac(a p^2).
-        float kzh = 0.f, kzl = 0.f, pz = 0.f, kxh = 0.f, kxl = 0.f, px = 0.f;
-        {
-            const double zr = va ? g.zp[iz] - g.oz : 0.0, xr = vb ? g.xp[ix] - g.ox : 0.0;
-            float unused;
+        const int q = p / kFRowThreads, rq = p % kFRowThreads;
+        bool va[kFRowsPer], vb[kFRowsPer];
+        // Per-row terms: kappa = -2 a p (hi, lo) and P = frac(a p^2), the A
+        // row in .x and the B row in .y.
+        float2 kh2[kFRowsPer], khn2[kFRowsPer], kl2[kFRowsPer], pp2[kFRowsPer];
+#pragma unroll
+        for (int k = 0; k < kFRowsPer; ++k) {
+            const int r = rq + kFRowThreads * k;
+            const size_t iz = (size_t)mt * 128 + r, ix = (size_t)nt * 128 + r;
+            va[k] = iz < g.nz;
+            vb[k] = ix < g.nx;
+            const double zr = va[k] ? g.zp[iz] - g.oz : 0.0, xr = vb[k] ? g.xp[ix] - g.ox : 0.0;
+            float kzh, kzl, kxh, kxl, pz, px, unused, h0, l0;
             split_coord(-2.0 * g.a_turns * zr, 0.0, &kzh, &kzl, &unused);
             split_coord(-2.0 * g.a_turns * xr, 0.0, &kxh, &kxl, &unused);
-            float h0, l0;
             split_coord(zr, g.a_turns, &h0, &l0, &pz);
             split_coord(xr, g.a_turns, &h0, &l0, &px);
+            kh2[k] = make_float2(kzh, kxh);
+            khn2[k] = make_float2(-kzh, -kxh);
+            kl2[k] = make_float2(kzl, kxl);
+            pp2[k] = make_float2(pz, px);
         }
-        const float2 kh2 = make_float2(kzh, kxh), khn2 = make_float2(-kzh, -kxh),
-                     kl2 = make_float2(kzl, kxl), pp2 = make_float2(pz, px);
-        auto stage = [&](int buf) { return reinterpret_cast<float4*>(rays_smem + buf * kFRayBytes); };
-        // Ray values of block `blk` (threads 0..31, one ray each). `fetch`
-        // only issues the loads, so that they are in flight during the
-        // block's phasors; `put` splits them and stages them as (z, x) pairs
-        // for the packed phase: {zh, xh, zl, xl}, {zf, xf, es_re, es_im}
-        // (amplitude scaled).
-        struct RawRay {
-            double x, z, er, ei;
-        };
-        auto fetch = [&](int blk, RawRay* v) {
-            const size_t j = (size_t)(rb0 + blk) * kFRays + p;
-            if (p >= 32) return;
-            if (j >= g.n) {
-                *v = RawRay{g.ox, g.oz, 0.0, 0.0};
-                return;
-            }
-            *v = RawRay{__ldg(g.rx + j), __ldg(g.rz + j), __ldg(g.er + j), __ldg(g.ei + j)};
-        };
-        auto put = [&](int buf, const RawRay& v) {
-            if (p < 32) {
-                float xh, xl, xf, zh, zl, zf;
-                split_coord(v.x - g.ox, g.a_turns, &xh, &xl, &xf);
-                split_coord(v.z - g.oz, g.a_turns, &zh, &zl, &zf);
-                stage(buf)[2 * p] = make_float4(zh, xh, zl, xl);
-                stage(buf)[2 * p + 1] = make_float4(zf, xf, (float)(v.er * g.inv_scale),
-                                                    (float)(v.ei * g.inv_scale));
-            }
-        };
-        if (nrb > 0) {
-            RawRay v;
-            fetch(0, &v);
-            put(0, v);
-        }
-        producer_sync();
         for (int i = 0; i < nrb; ++i) {
-            const int s = i % kFStages, rbuf = i & 1;
-            RawRay nxt{g.ox, g.oz, 0.0, 0.0};
-            if (i + 1 < nrb) fetch(i + 1, &nxt);  // in flight during this block
-            if (!mbar_wait(&empty[s], ((uint32_t)(i / kFStages) & 1u) ^ 1u, g.wait_limit)) *flag = 1;
+            const int s = i % kFStages, rb = i % kFRayBufs;
+            bool ok = mbar_wait(&ray_full[rb], (uint32_t)(i / kFRayBufs) & 1u, g.wait_limit);
+            ok = mbar_wait(&empty[s], ((uint32_t)(i / kFStages) & 1u) ^ 1u, g.wait_limit) && ok;
+            if (!ok) *flag = 1;
             unsigned char* base = tiles + (size_t)s * kFStage;
-            const float4* sr = stage(rbuf);
+            const float4* sr = reinterpret_cast<const float4*>(rays_smem + rb * kFRayBytes);
 #pragma unroll 1
-            for (int cc = 0; cc < 4; ++cc) {
-                const int c = 4 * h + cc;
-                uint32_t ah[4], al[4], bh[4], bl[4];
+            for (int cc = 0; cc < kFChunks; ++cc) {
+                const int c = kFChunks * q + cc;
+                uint32_t ah[kFRowsPer][4], al[kFRowsPer][4], bh[kFRowsPer][4], bl[kFRowsPer][4];
 #pragma unroll
                 for (int jj = 0; jj < 4; ++jj) {
                     const int j = 4 * c + jj;
                     const float4 v0 = sr[2 * j], v1 = sr[2 * j + 1];
-                    // Phase in turns of the A row (.x) and the B row (.y).
-                    const float2 t = pair_turns2(kh2, khn2, kl2,
-                                                 __fadd2_rn(pp2, make_float2(v1.x, v1.y)),
-                                                 make_float2(v0.x, v0.y), make_float2(v0.z, v0.w));
-                    const float2 th = __fmul2_rn(t, f2(6.28318530717958647692f));
-                    float ca, sa, cb, sb, wr = 0.f, wi = 0.f;
-                    __sincosf(th.x, &sa, &ca);
-                    __sincosf(th.y, &sb, &cb);
-                    if (!va) ca = sa = 0.f;
-                    if (vb) {
-                        wr = v1.z * cb - v1.w * sb;
-                        wi = v1.z * sb + v1.w * cb;
+#pragma unroll
+                    for (int k = 0; k < kFRowsPer; ++k) {
+                        // Phase in turns of the A row (.x) and the B row (.y).
+                        const float2 t = pair_turns2(kh2[k], khn2[k], kl2[k],
+                                                     __fadd2_rn(pp2[k], make_float2(v1.x, v1.y)),
+                                                     make_float2(v0.x, v0.y),
+                                                     make_float2(v0.z, v0.w));
+                        const float2 th = __fmul2_rn(t, f2(6.28318530717958647692f));
+                        float ca, sa, cb, sb, wr = 0.f, wi = 0.f;
+                        __sincosf(th.x, &sa, &ca);
+                        __sincosf(th.y, &sb, &cb);
+                        if (!va[k]) ca = sa = 0.f;
+                        if (vb[k]) {
+                            wr = v1.z * cb - v1.w * sb;
+                            wi = v1.z * sb + v1.w * cb;
+                        }
+                        split16x2(ca, sa, &ah[k][jj], &al[k][jj]);
+                        split16x2(wr, wi, &bh[k][jj], &bl[k][jj]);
                     }
-                    split16x2(ca, sa, &ah[jj], &al[jj]);
-                    split16x2(wr, wi, &bh[jj], &bl[jj]);
                 }
-                // A row: (Re Z, Im Z); B rows 2r: (Re W, -Im W), 2r+1: (Im W, Re W).
-                *reinterpret_cast<uint4*>(base + sw128(r, c)) = make_uint4(ah[0], ah[1], ah[2], ah[3]);
-                *reinterpret_cast<uint4*>(base + kFA + sw128(r, c)) =
-                    make_uint4(al[0], al[1], al[2], al[3]);
                 unsigned char* bhi = base + 2 * kFA;
                 unsigned char* blo = bhi + kFB;
-                // Rows 2r and 2r+1. Eight consecutive threads' stores to even
-                // rows meet four swizzle phases (a 2-way conflict); ordering
-                // the two stores per thread to spread them cost 16 selects
-                // per chunk and was 1.5 % slower overall.
-                const uint4 e0h = make_uint4(neg_hi(bh[0]), neg_hi(bh[1]), neg_hi(bh[2]), neg_hi(bh[3]));
-                const uint4 e1h = make_uint4(swap_halves(bh[0]), swap_halves(bh[1]),
-                                             swap_halves(bh[2]), swap_halves(bh[3]));
-                const uint4 e0l = make_uint4(neg_hi(bl[0]), neg_hi(bl[1]), neg_hi(bl[2]), neg_hi(bl[3]));
-                const uint4 e1l = make_uint4(swap_halves(bl[0]), swap_halves(bl[1]),
-                                             swap_halves(bl[2]), swap_halves(bl[3]));
-                *reinterpret_cast<uint4*>(bhi + sw128(2 * r, c)) = e0h;
-                *reinterpret_cast<uint4*>(bhi + sw128(2 * r + 1, c)) = e1h;
-                *reinterpret_cast<uint4*>(blo + sw128(2 * r, c)) = e0l;
-                *reinterpret_cast<uint4*>(blo + sw128(2 * r + 1, c)) = e1l;
+#pragma unroll
+                for (int k = 0; k < kFRowsPer; ++k) {
+                    const uint32_t r = (uint32_t)(rq + kFRowThreads * k);
+                    // A row: (Re Z, Im Z); B rows r: (Re W, -Im W), 128 + r:
+                    // (Im W, Re W). Each store instruction writes 32
+                    // consecutive rows, which meet all eight swizzle phases
+                    // (no bank conflict).
+                    *reinterpret_cast<uint4*>(base + sw128(r, c)) =
+                        make_uint4(ah[k][0], ah[k][1], ah[k][2], ah[k][3]);
+                    *reinterpret_cast<uint4*>(base + kFA + sw128(r, c)) =
+                        make_uint4(al[k][0], al[k][1], al[k][2], al[k][3]);
+                    *reinterpret_cast<uint4*>(bhi + sw128(r, c)) =
+                        make_uint4(neg_hi(bh[k][0]), neg_hi(bh[k][1]), neg_hi(bh[k][2]), neg_hi(bh[k][3]));
+                    *reinterpret_cast<uint4*>(bhi + sw128(128 + r, c)) =
+                        make_uint4(swap_halves(bh[k][0]), swap_halves(bh[k][1]),
+                                   swap_halves(bh[k][2]), swap_halves(bh[k][3]));
+                    *reinterpret_cast<uint4*>(blo + sw128(r, c)) =
+                        make_uint4(neg_hi(bl[k][0]), neg_hi(bl[k][1]), neg_hi(bl[k][2]), neg_hi(bl[k][3]));
+                    *reinterpret_cast<uint4*>(blo + sw128(128 + r, c)) =
+                        make_uint4(swap_halves(bl[k][0]), swap_halves(bl[k][1]),
+                                   swap_halves(bl[k][2]), swap_halves(bl[k][3]));
+                }
             }
             // Make the generic-proxy stores visible to the tensor cores, then
             // one arrival per warp.
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(&full[s]);
-            if (i + 1 < nrb) put(rbuf ^ 1, nxt);
-            producer_sync();
+            if (lane == 0) {
+                mbar_arrive(&full[s]);
+                mbar_arrive(&ray_empty[rb]);
+            }
+        }
+    } else {
+        // Ray stager: lane l stages ray l of each block as (z, x) pairs for
+        // the packed phase: {zh, xh, zl, xl}, {zf, xf, es_re, es_im}
+        // (coordinates relative to the screen centre, amplitude scaled). The
+        // next block's loads are in flight while the stager waits for its
+        // buffer to be released.
+        for (int i = 0; i < nrb; ++i) {
+            const int rb = i % kFRayBufs;
+            const size_t j = (size_t)(rb0 + i) * kFRays + lane;
+            double x = g.ox, z = g.oz, er = 0.0, ei = 0.0;
+            if (j < g.n) {
+                x = __ldg(g.rx + j);
+                z = __ldg(g.rz + j);
+                er = __ldg(g.er + j);
+                ei = __ldg(g.ei + j);
+            }
+            if (i >= kFRayBufs &&
+                !mbar_wait(&ray_empty[rb], (uint32_t)(i / kFRayBufs - 1) & 1u, g.wait_limit))
+                *flag = 1;
+            float xh, xl, xf, zh, zl, zf;
+            split_coord(x - g.ox, g.a_turns, &xh, &xl, &xf);
+            split_coord(z - g.oz, g.a_turns, &zh, &zl, &zf);
+            float4* st = reinterpret_cast<float4*>(rays_smem + rb * kFRayBytes);
+            st[2 * lane] = make_float4(zh, xh, zl, xl);
+            st[2 * lane + 1] = make_float4(zf, xf, (float)(er * g.inv_scale), (float)(ei * g.inv_scale));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ray_full[rb]);
         }
     }
     __syncthreads();
@@ -453,7 +482,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
     }
 }
 
-// acc[iz*nx + ix] (+)= scale * sum over splits of C[iz][2ix + c], in FP64 and
+// acc[iz*nx + ix] (+)= scale * sum over splits of C[iz][n(ix, c)], in FP64 and
 // split order.
 // The ray set's bounds the product needs before it starts: max |es_re|,
 // |es_im| (the f16 scaling), max |x - ox| and |z - oz| (the cross-term bound),
@@ -502,10 +531,9 @@ __global__ void reduce_kernel(const double* __restrict__ partial, int splits, in
     const size_t iz = idx / nx, ix = idx - iz * nx;
     double re = 0.0, im = 0.0;
     for (int s = 0; s < splits; ++s) {
-        const double2 v = *reinterpret_cast<const double2*>(
-            partial + ((size_t)s * m_pad + iz) * n_pad + 2 * ix);
-        re += v.x;
-        im += v.y;
+        const double* row = partial + ((size_t)s * m_pad + iz) * n_pad + (ix >> 7) * kFN + (ix & 127);
+        re += row[0];
+        im += row[128];
     }
     re *= scale;
     im *= scale;
