@@ -54,6 +54,9 @@ SFU_OPS_PER_PAIR = 4
 # 512^2 workload from an ncu capture of the full-size launch, by the number of
 # amplitude columns summed (two-column kernel: key False).
 DRAM_BYTES_CONFIG1 = {False: 502.3e6, True: 270.7e6}
+# The same for one fresnel_pair_kernel launch on 2^20 rays x 512^2: the four
+# ray columns read once (the FP64 split partials stay in L2).
+FRESNEL_DRAM_BYTES_CONFIG = 33.8e6
 
 
 def parse():
@@ -509,10 +512,13 @@ def run_fresnel(args):
                        "this pool (MEASURED_PEAKS.json absent; f16 runs at the bf16 rate)")
     gemm = float(np.mean(gemm_ms))
     achieved = algo_flops / (gemm / 1e3) / 1e12
-    # DRAM bytes (read + write) of one fresnel_fused_kernel launch on the
+    # Screens of more than 128 rows run on CTA pairs (stats sweep = 1).
+    fr_kernel = "fresnel_pair_kernel" if st["sweep"] == 1 else "fresnel_fused_kernel"
+    # DRAM bytes (read + write) of one fresnel_pair_kernel launch on the
     # 2^20-ray 512x512 workload, from a single-pass ncu capture of full-size
     # launches; other sizes report null.
-    fr_traffic = 33.8e6 if (args.rays == 1 << 20 and args.grid == 512) else None
+    fr_traffic = (FRESNEL_DRAM_BYTES_CONFIG
+                  if (args.rays == 1 << 20 and args.grid == 512 and st["sweep"] == 1) else None)
     cpu = None
     if not args.no_cpu:
         row = xrt_rs.FresnelScreen(-0.5, 0.5, g, 0.0, 0.0, 1)
@@ -540,7 +546,7 @@ def run_fresnel(args):
                         "ms_per_step": st64["gpu_ms"],
                         "speedup_separable_vs_f64": st64["gpu_ms"] / dev,
                         "rel_l2_separable_vs_f64": err},
-        "roofline": {"bound": "tensor", "kernel": "fresnel_fused_kernel",
+        "roofline": {"bound": "tensor", "kernel": fr_kernel,
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": fr_traffic, "kernel_ms": gemm,
                      "peak_source": peak_source,

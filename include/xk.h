@@ -108,7 +108,8 @@ typedef struct xk_stats {
     int groups;              /* ray groups per tile (F32PR) */
     int routed_reason;       /* 0 = not routed; see xk_route_reason() */
     int sweep;               /* F32PR sweep used: 0 SFU reciprocal, 1 packed + quadratic series,
-                                2 packed + linear series, -1 none */
+                                2 packed + linear series; XK_PATH_SEPARABLE (Fresnel): 1 CTA-pair
+                                tiles, 0 one CTA per tile; -1 none */
     int one_polarization;    /* F32PR: 1 if every ray had ray 0's polarization, so the kernel
                                 summed one amplitude column and Ep = (ep_0 / es_0) Es */
     int tuned;               /* F32PR: 1 if the solve used autotuned settings of its bucket */
@@ -173,7 +174,10 @@ const char* xk_route_reason(int reason);
  *                    context arms its first ray stage's barrier with this many
  *                    bytes (a positive multiple of 16, at most 1024) beyond its
  *                    copy, so that stage can never complete and the bounded
- *                    wait runs out; cleared after that one execution */
+ *                    wait runs out; cleared after that one execution
+ *   "fresnel_pair"   XK_PATH_SEPARABLE: 1 (default) computes screens of more
+ *                    than 128 rows on CTA pairs (one tcgen05 MMA over two SMs,
+ *                    256 x 256 tiles); 0 keeps one CTA per 128 x 256 tile */
 int xk_set_option(xk_ctx* ctx, const char* name, double value);
 
 typedef struct xk_tune_result {

@@ -126,6 +126,28 @@ def test_empty_screen_and_bad_arguments(ctx):
                                  FresnelScreen(-1, 1, 2, -1, 1, 2), path="f32", ctx=ctx)
 
 
+@pytest.mark.parametrize("shape", [(300, 200), (129, 257), (64, 384)])
+def test_cta_pair_tiles_match_single_cta_tiles(ctx, oracle, shape):
+    """Screens of more than 128 rows run the product on CTA pairs (one tcgen05
+    MMA over two SMs, 256 x 256 tiles, option "fresnel_pair" = 1, the
+    default); "fresnel_pair" = 0 keeps one CTA per 128 x 256 tile. Both match
+    the oracle, and each other to within the f32 accumulation order."""
+    nx, nz = shape
+    x, z, es = rays(3000, seed=31 + nx)
+    sc = FresnelScreen(-0.3, 0.3, nx, -0.25, 0.2, nz)
+    pair = xrt_rs.fresnel_propagate(x, z, es, 10000.0, 1000.0, sc, ctx=ctx).amplitude
+    ctx.set_option("fresnel_pair", 0)
+    try:
+        single = xrt_rs.fresnel_propagate(x, z, es, 10000.0, 1000.0, sc, ctx=ctx).amplitude
+    finally:
+        ctx.set_option("fresnel_pair", 1)
+    ref = oracle_field(oracle, x, z, es, 10000.0, 1000.0, sc)
+    e_pair, e_single, e_both = rel(pair, ref), rel(single, ref), rel(pair, single)
+    print(f"{nx}x{nz}: pair {e_pair:.2e}, single {e_single:.2e}, pair vs single {e_both:.2e}")
+    assert e_pair < SEP_TOL and e_single < SEP_TOL
+    assert e_both < 1e-6
+
+
 def test_separable_long_accumulation_against_f64(ctx):
     """Few K splits per output tile (a 1024x1024 screen has 64 tiles), so each
     CTA accumulates ~900 K blocks: the segmented FP64 drain keeps the product

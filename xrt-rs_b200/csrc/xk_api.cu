@@ -351,6 +351,9 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
             return fail(ctx, XK_ERR_INVALID, "wait_limit must be an integer in 1..2^31");
         ctx->prws.ctl.wait_limit = (uint32_t)value;
         ctx->fresnel.wait_limit = (uint32_t)value;
+    } else if (n == "fresnel_pair") {
+        if (value != 0.0 && value != 1.0) return fail(ctx, XK_ERR_INVALID, "fresnel_pair is 0 or 1");
+        ctx->fresnel.allow_pair = value != 0.0;
     } else if (n == "inject_stall") {
         if (!(value >= 0.0) || value > 1024.0 || std::fmod(value, 16.0) != 0.0)
             return fail(ctx, XK_ERR_INVALID, "inject_stall must be a multiple of 16 in 0..1024");

@@ -135,8 +135,10 @@ constexpr int kFN = 256;                         // accumulator columns (N of th
 // z lo, frac(a z^2) (coordinates relative to the screen centre) and the
 // scaled amplitude.
 constexpr uint32_t kFRayBytes = kFRays * 32;
-// Epilogue transpose buffers: per epilogue warp 32 x 33 floats.
-constexpr uint32_t kFEpiBytes = 4 * 32 * 33 * 4;
+// Epilogue staging: per epilogue warp 32 rows of 16 FP64 values, rows 144
+// bytes apart (16-byte stores of 32 lanes then meet all banks once).
+constexpr uint32_t kFEpiRow = 144;
+constexpr uint32_t kFEpiBytes = 4 * 32 * kFEpiRow;
 constexpr size_t kFSmem = 1024 + (size_t)kFStages * kFStage + kFRayBufs * kFRayBytes + kFEpiBytes + 256;
 
 struct FusedArgs {
@@ -214,6 +216,100 @@ __device__ __forceinline__ void split16x2(float a, float b, uint32_t* hi, uint32
 __device__ __forceinline__ uint32_t neg_hi(uint32_t v) { return v ^ 0x80000000u; }
 __device__ __forceinline__ uint32_t swap_halves(uint32_t v) { return __byte_perm(v, 0, 0x1032); }
 
+// Epilogue role (warps 1..4): drains each finished accumulator segment into
+// this CTA's 128 rows of the FP64 split partial; `arrive_empty(b)` releases
+// accumulator b to the MMA issuer. Warp w reads TMEM lanes 32 (w % 4) .. + 31
+// (rows qd*32 .. +31 of the tile); lane l owns row qd*32 + l. Per 16-column
+// chunk the lane converts its values to FP64 in its shared-memory staging row
+// and hands the row to a bulk copy: the first segment stores it, later ones
+// add it to the partial at the memory side (FP64 add, round to nearest). A
+// segment's operations complete before the next segment's start, so the
+// partial is s0 + s1 + ... in segment order, independent of timing. `stage`:
+// this warp's 32 staging rows.
+template <class ArriveEmpty>
+__device__ __forceinline__ void drain_role(const FusedArgs& g, int warp, int lane, int mt, int nt,
+                                           int sp, int nseg, uint32_t tmem, uint64_t* acc_full,
+                                           unsigned char* stage, volatile int* flag,
+                                           ArriveEmpty arrive_empty) {
+    using namespace sm100;
+    const int qd = warp & 3;
+    if (nseg == 0) {
+        double* rows0 = g.partial + ((size_t)sp * g.m_pad + (size_t)mt * 128 + qd * 32) * g.n_pad +
+                        (size_t)nt * kFN + lane;
+        for (int rr = 0; rr < 32; ++rr)
+            for (int c = 0; c < kFN; c += 32) rows0[(size_t)rr * g.n_pad + c] = 0.0;
+        return;
+    }
+    double* grow = g.partial + ((size_t)sp * g.m_pad + (size_t)mt * 128 + qd * 32 + lane) * g.n_pad +
+                   (size_t)nt * kFN;
+    unsigned char* srow = stage + lane * kFEpiRow;
+    const uint32_t s_addr = smem_u32(srow);
+    for (int q = 0; q < nseg; ++q) {
+        const int b = q & 1;
+        const bool ok = mbar_wait(&acc_full[b], (uint32_t)(q >> 1) & 1u, g.wait_limit);
+        if (!__all_sync(0xffffffffu, ok)) {
+            *flag = 1;
+            break;
+        }
+        tc_fence_after();
+        bulk_wait_all();  // the previous segment's writes to these rows are performed
+#pragma unroll 1
+        for (int c = 0; c < kFN / 16; ++c) {
+            float v[16];
+            tmem_ld_16cols(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * kFN + c * 16), v);
+            bulk_wait_read();  // the staging row is free again
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                reinterpret_cast<double2*>(srow)[k] =
+                    make_double2((double)v[2 * k], (double)v[2 * k + 1]);
+            fence_proxy_async();
+            if (q == 0)
+                bulk_s2g(grow + c * 16, s_addr, 128);
+            else
+                bulk_add_s2g_f64(grow + c * 16, s_addr, 128);
+            bulk_commit();
+        }
+        tc_fence_before();
+        arrive_empty(b);
+    }
+    bulk_wait_all();
+}
+
+// Ray stager role (one warp): stages the ray blocks rb0 .. rb0 + nrb - 1 in a
+// ring of kFRayBufs shared-memory buffers.
+__device__ __forceinline__ void stage_rays_role(const FusedArgs& g, int lane, int rb0, int nrb,
+                                                unsigned char* rays_smem, uint64_t* ray_full,
+                                                uint64_t* ray_empty, volatile int* flag) {
+    using namespace sm100;
+    // Ray stager: lane l stages ray l of each block as (z, x) pairs for
+    // the packed phase: {zh, xh, zl, xl}, {zf, xf, es_re, es_im}
+    // (coordinates relative to the screen centre, amplitude scaled). The
+    // next block's loads are in flight while the stager waits for its
+    // buffer to be released.
+    for (int i = 0; i < nrb; ++i) {
+        const int rb = i % kFRayBufs;
+        const size_t j = (size_t)(rb0 + i) * kFRays + lane;
+        double x = g.ox, z = g.oz, er = 0.0, ei = 0.0;
+        if (j < g.n) {
+            x = __ldg(g.rx + j);
+            z = __ldg(g.rz + j);
+            er = __ldg(g.er + j);
+            ei = __ldg(g.ei + j);
+        }
+        if (i >= kFRayBufs &&
+            !mbar_wait(&ray_empty[rb], (uint32_t)(i / kFRayBufs - 1) & 1u, g.wait_limit))
+            *flag = 1;
+        float xh, xl, xf, zh, zl, zf;
+        split_coord(x - g.ox, g.a_turns, &xh, &xl, &xf);
+        split_coord(z - g.oz, g.a_turns, &zh, &zl, &zf);
+        float4* st = reinterpret_cast<float4*>(rays_smem + rb * kFRayBytes);
+        st[2 * lane] = make_float4(zh, xh, zl, xl);
+        st[2 * lane + 1] = make_float4(zf, xf, (float)(er * g.inv_scale), (float)(ei * g.inv_scale));
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ray_full[rb]);
+    }
+}
+
 __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g) {
     using namespace sm100;
     extern __shared__ unsigned char smem_raw[];
@@ -225,9 +321,11 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* ray_full = acc_empty + 2;
     uint64_t* ray_empty = ray_full + kFRayBufs;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ray_empty + kFRayBufs);
+    uint64_t* mma_done = ray_empty + kFRayBufs;  // every issued MMA has completed
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
     volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    unsigned char* rays_smem = reinterpret_cast<unsigned char*>(tmem_slot) + 64;
+    unsigned char* rays_smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(tmem_slot) + 64 + 15) & ~static_cast<uintptr_t>(15));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = blockIdx.x, nt = blockIdx.y, sp = blockIdx.z;
@@ -249,6 +347,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             mbar_init(&ray_full[b], 1);                      // the stager warp
             mbar_init(&ray_empty[b], kFProdThreads / 32);  // one arrival per producer warp
         }
+        mbar_init(mma_done, 1);
         mbar_init_fence();
         *flag = 0;
     }
@@ -295,53 +394,16 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
                 }
                 umma_commit(&acc_full[b]);
             }
+            // A loop that gave up on a wait may leave MMAs in flight: wait
+            // (bounded) for them before the accumulators are freed.
+            umma_commit(mma_done);
+            if (!mbar_wait(mma_done, 0, g.wait_limit)) *flag = 1;
         }
         __syncwarp();
     } else if (warp <= 4) {
-        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, i.e. rows
-        // qd*32 .. +31 of the tile. Each 32 x 32 block of the accumulator is
-        // transposed through shared memory so that the FP64 partial is
-        // updated one row at a time, 32 consecutive columns per access.
-        const int qd = warp & 3;
-        float* tb = reinterpret_cast<float*>(rays_smem + kFRayBufs * kFRayBytes) + (warp - 1) * 32 * 33;
-        double* rows0 = g.partial + ((size_t)sp * g.m_pad + (size_t)mt * 128 + qd * 32) * g.n_pad +
-                        (size_t)nt * kFN + lane;
-        if (nseg == 0)
-            for (int rr = 0; rr < 32; ++rr)
-                for (int c = 0; c < kFN; c += 32) rows0[(size_t)rr * g.n_pad + c] = 0.0;
-        for (int q = 0; q < nseg; ++q) {
-            const int b = q & 1;
-            const bool ok = mbar_wait(&acc_full[b], (uint32_t)(q >> 1) & 1u, g.wait_limit);
-            if (!__all_sync(0xffffffffu, ok)) {
-                *flag = 1;
-                break;
-            }
-            tc_fence_after();
-#pragma unroll 1
-            for (int c = 0; c < kFN / 32; ++c) {
-                float v[32];
-                tmem_ld_32cols(tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * kFN + c * 32), v);
-#pragma unroll
-                for (int k = 0; k < 32; ++k) tb[lane * 33 + k] = v[k];
-                __syncwarp();
-                double* d = rows0 + c * 32;
-                if (q == 0) {
-#pragma unroll
-                    for (int rr = 0; rr < 32; ++rr) d[(size_t)rr * g.n_pad] = (double)tb[rr * 33 + lane];
-                } else {
-                    // All 32 loads in flight before the adds.
-                    double old[32];
-#pragma unroll
-                    for (int rr = 0; rr < 32; ++rr) old[rr] = d[(size_t)rr * g.n_pad];
-#pragma unroll
-                    for (int rr = 0; rr < 32; ++rr)
-                        d[(size_t)rr * g.n_pad] = old[rr] + (double)tb[rr * 33 + lane];
-                }
-                __syncwarp();
-            }
-            tc_fence_before();
-            mbar_arrive(&acc_empty[b]);
-        }
+        unsigned char* tb = rays_smem + kFRayBufs * kFRayBytes + (warp - 1) * 32 * kFEpiRow;
+        drain_role(g, warp, lane, mt, nt, sp, nseg, tmem, acc_full, tb, flag,
+                   [&](int b) { mbar_arrive(&acc_empty[b]); });
     } else if (warp < 5 + kFProdThreads / 32) {
         // Producers: thread p owns kFRowsPer A rows r_k = (p % kFRowThreads) +
         // kFRowThreads k (screen z index mt*128 + r_k) and the B rows r_k,
@@ -444,33 +506,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             }
         }
     } else {
-        // Ray stager: lane l stages ray l of each block as (z, x) pairs for
-        // the packed phase: {zh, xh, zl, xl}, {zf, xf, es_re, es_im}
-        // (coordinates relative to the screen centre, amplitude scaled). The
-        // next block's loads are in flight while the stager waits for its
-        // buffer to be released.
-        for (int i = 0; i < nrb; ++i) {
-            const int rb = i % kFRayBufs;
-            const size_t j = (size_t)(rb0 + i) * kFRays + lane;
-            double x = g.ox, z = g.oz, er = 0.0, ei = 0.0;
-            if (j < g.n) {
-                x = __ldg(g.rx + j);
-                z = __ldg(g.rz + j);
-                er = __ldg(g.er + j);
-                ei = __ldg(g.ei + j);
-            }
-            if (i >= kFRayBufs &&
-                !mbar_wait(&ray_empty[rb], (uint32_t)(i / kFRayBufs - 1) & 1u, g.wait_limit))
-                *flag = 1;
-            float xh, xl, xf, zh, zl, zf;
-            split_coord(x - g.ox, g.a_turns, &xh, &xl, &xf);
-            split_coord(z - g.oz, g.a_turns, &zh, &zl, &zf);
-            float4* st = reinterpret_cast<float4*>(rays_smem + rb * kFRayBytes);
-            st[2 * lane] = make_float4(zh, xh, zl, xl);
-            st[2 * lane + 1] = make_float4(zf, xf, (float)(er * g.inv_scale), (float)(ei * g.inv_scale));
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&ray_full[rb]);
-        }
+        stage_rays_role(g, lane, rb0, nrb, rays_smem, ray_full, ray_empty, flag);
     }
     __syncthreads();
     if (*flag != 0 && threadIdx.x == 0) atomicExch(g.err, 1);
@@ -479,6 +515,266 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
     if (warp == 0) {
         tc_fence_after();
         tmem_free(tmem, 2 * kFN);
+    }
+}
+
+// ---- the same product on CTA pairs (tcgen05 cta_group::2) ---------------------
+//
+// A cluster of two CTAs computes a 256 x 256 accumulator tile (256 z rows, 128
+// x points) with one pair MMA per K step, issued by the even CTA: each CTA
+// holds its 128 A rows and half of B (64 x points: their real parts in local
+// rows 0..63, their imaginary parts in 64..127), and each keeps its 128
+// accumulator rows in its own TMEM. Per 32-ray block a CTA therefore computes
+// 128 A and 64 B phasors per ray instead of 128 + 128, stores 64 KB of tiles
+// instead of 96 KB, and its tensor core reads half of B from each CTA. The
+// accumulator column of x point ix is n = 128 h + 64 c + ix % 64 with
+// h = (ix % 128) / 64 (the CTA that holds it) and c = 0 (real), 1 (imaginary).
+constexpr int kPStages = 3;
+constexpr uint32_t kPA = 128 * 128;              // one A tile (hi or lo): 128 rows x 128 B
+constexpr uint32_t kPB = 128 * 128;              // this CTA's half of one B tile
+constexpr uint32_t kPStage = 2 * kPA + 2 * kPB;  // A_hi | A_lo | B_hi | B_lo
+constexpr int kPProdThreads = 256;               // warps 5..12
+constexpr int kPThreads = 32 + kFEpiThreads + kPProdThreads + 32;
+constexpr size_t kPSmem =
+    1024 + (size_t)kPStages * kPStage + kFRayBufs * kFRayBytes + kFEpiBytes + 256;
+static_assert(kPSmem <= 227 * 1024, "pair kernel shared memory");
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    fresnel_pair_kernel(FusedArgs g) {
+    using namespace sm100;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* tiles = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(tiles + kPStages * kPStage);
+    uint64_t* empty = full + kPStages;
+    uint64_t* acc_full = empty + kPStages;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* ray_full = acc_empty + 2;
+    uint64_t* ray_empty = ray_full + kFRayBufs;
+    uint64_t* mma_done = ray_empty + kFRayBufs;  // every issued MMA has completed
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+    volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    unsigned char* rays_smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(tmem_slot) + 64 + 15) & ~static_cast<uintptr_t>(15));
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mt = blockIdx.x, nt = blockIdx.y, sp = blockIdx.z;
+    const uint32_t half = cluster_ctarank(), peer = half ^ 1u;
+    const bool leader = half == 0;
+    const int rb0 = (int)((long long)g.ray_blocks * sp / g.splits);
+    const int rb1 = (int)((long long)g.ray_blocks * (sp + 1) / g.splits);
+    const int nrb = rb1 - rb0;
+    const int nseg = (nrb + kFSeg - 1) / kFSeg;
+
+    if (threadIdx.x == 0) {
+        // full and acc_empty are used in the even CTA only: they collect the
+        // arrivals of both CTAs' producer and epilogue warps.
+        for (int s = 0; s < kPStages; ++s) {
+            mbar_init(&full[s], 2 * kPProdThreads / 32);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 2 * kFEpiThreads);
+        }
+        for (int b = 0; b < kFRayBufs; ++b) {
+            mbar_init(&ray_full[b], 1);
+            mbar_init(&ray_empty[b], kPProdThreads / 32);
+        }
+        mbar_init(mma_done, 1);
+        mbar_init_fence();
+        *flag = 0;
+    }
+    if (warp == 0) tmem_alloc_pair(tmem_slot, 2 * kFN);
+    tc_fence_before();
+    cluster_sync();  // both CTAs' barriers initialised, TMEM allocated in both
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (leader && lane == 0) {
+            // Pair MMA issuer: per ray block three K blocks (hi.hi, hi.lo,
+            // lo.hi) of four 256x256x16 steps; segment q accumulates into
+            // buffer q & 1 of both CTAs' TMEM.
+            constexpr uint32_t idesc = idesc_f16_f32(256, kFN);
+            bool good = true;
+            for (int q = 0; q < nseg && good; ++q) {
+                const int b = q & 1, use = q >> 1;
+                if (use >= 1 &&
+                    !mbar_wait_cluster(&acc_empty[b], (uint32_t)(use - 1) & 1u, g.wait_limit)) {
+                    *flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(b * kFN);
+                const int i0 = q * kFSeg, i1 = min(nrb, i0 + kFSeg);
+                for (int i = i0; i < i1; ++i) {
+                    const int s = i % kPStages;
+                    if (!mbar_wait_cluster(&full[s], (uint32_t)(i / kPStages) & 1u, g.wait_limit)) {
+                        *flag = 1;
+                        good = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_hi = smem_u32(tiles + (size_t)s * kPStage);
+                    const uint32_t a_lo = a_hi + kPA, b_hi = a_hi + 2 * kPA, b_lo = b_hi + kPB;
+                    const uint32_t as[3] = {a_hi, a_hi, a_lo}, bs[3] = {b_hi, b_lo, b_hi};
+#pragma unroll
+                    for (int p = 0; p < 3; ++p)
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            umma_f16_pair(d, desc_kmajor_sw128(as[p] + 32u * k),
+                                          desc_kmajor_sw128(bs[p] + 32u * k), idesc,
+                                          (uint32_t)((i - i0) | p | k));
+                    umma_commit_pair(smem_u32(&empty[s]));
+                    umma_commit_pair(mapa_shared(&empty[s], peer));
+                }
+                umma_commit_pair(smem_u32(&acc_full[b]));
+                umma_commit_pair(mapa_shared(&acc_full[b], peer));
+            }
+            // A loop that gave up on a wait may leave MMAs in flight: wait
+            // (bounded) for them before either CTA frees its accumulators.
+            umma_commit_pair(smem_u32(mma_done));
+            if (!mbar_wait(mma_done, 0, g.wait_limit)) *flag = 1;
+        }
+        __syncwarp();
+    } else if (warp <= 4) {
+        unsigned char* tb = rays_smem + kFRayBufs * kFRayBytes + (warp - 1) * 32 * kFEpiRow;
+        const uint32_t acc_empty_lead = mapa_shared(acc_empty, 0);
+        drain_role(g, warp, lane, mt, nt, sp, nseg, tmem, acc_full, tb, flag, [&](int b) {
+            mbar_arrive_cluster(acc_empty_lead + 8u * (uint32_t)b);
+        });
+    } else if (warp < 5 + kPProdThreads / 32) {
+        // Producers: warp w' = warp - 5 fills 16-byte chunk c = w' (rays
+        // 4c .. 4c+3) of every row; lane l computes the A rows l, l + 32,
+        // 64 + l, 96 + l (screen z index mt*128 + row) and the x points l,
+        // l + 32 of this CTA's half (screen x index nt*128 + 64 half + point).
+        // Three packed phase evaluations per ray: (A l, B l), (A l+32, B l+32)
+        // and (A 64+l, A 96+l). Each store instruction of a warp covers 32
+        // consecutive rows (no bank conflict).
+        const int c = warp - 5;
+        const int r = lane;
+        bool va[4], vb[2];
+        float2 kh2[3], khn2[3], kl2[3], pp2[3];
+        {
+            double zr[4], xr[2];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const size_t iz = (size_t)mt * 128 + r + 32 * k;
+                va[k] = iz < g.nz;
+                zr[k] = va[k] ? g.zp[iz] - g.oz : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const size_t ix = (size_t)nt * 128 + 64 * half + r + 32 * k;
+                vb[k] = ix < g.nx;
+                xr[k] = vb[k] ? g.xp[ix] - g.ox : 0.0;
+            }
+            // Pair-row e: (.x, .y) = (z row, x point) for e = 0, 1 and (z row,
+            // z row) for e = 2.
+            const double ux[3] = {zr[0], zr[1], zr[2]}, uy[3] = {xr[0], xr[1], zr[3]};
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                float hx, lx, hy, ly, fx, fy, unused, h0, l0;
+                split_coord(-2.0 * g.a_turns * ux[e], 0.0, &hx, &lx, &unused);
+                split_coord(-2.0 * g.a_turns * uy[e], 0.0, &hy, &ly, &unused);
+                split_coord(ux[e], g.a_turns, &h0, &l0, &fx);
+                split_coord(uy[e], g.a_turns, &h0, &l0, &fy);
+                kh2[e] = make_float2(hx, hy);
+                khn2[e] = make_float2(-hx, -hy);
+                kl2[e] = make_float2(lx, ly);
+                pp2[e] = make_float2(fx, fy);
+            }
+        }
+        const uint32_t full_lead = mapa_shared(full, 0);
+        for (int i = 0; i < nrb; ++i) {
+            const int s = i % kPStages, rb = i % kFRayBufs;
+            bool ok = mbar_wait(&ray_full[rb], (uint32_t)(i / kFRayBufs) & 1u, g.wait_limit);
+            ok = mbar_wait(&empty[s], ((uint32_t)(i / kPStages) & 1u) ^ 1u, g.wait_limit) && ok;
+            if (!ok) *flag = 1;
+            unsigned char* base = tiles + (size_t)s * kPStage;
+            const float4* sr = reinterpret_cast<const float4*>(rays_smem + rb * kFRayBytes);
+            uint32_t ah[4][4], al[4][4], bh[2][4], bl[2][4];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const int j = 4 * c + jj;
+                const float4 v0 = sr[2 * j], v1 = sr[2 * j + 1];
+                // Ray terms of the (z, x) and (z, z) pair-rows.
+                const float2 rh_zx = make_float2(v0.x, v0.y), rl_zx = make_float2(v0.z, v0.w);
+                const float2 rf_zx = make_float2(v1.x, v1.y);
+                const float2 rh_zz = f2(v0.x), rl_zz = f2(v0.z), rf_zz = f2(v1.x);
+#pragma unroll
+                for (int e = 0; e < 3; ++e) {
+                    const bool zz = e == 2;
+                    const float2 t = pair_turns2(kh2[e], khn2[e], kl2[e],
+                                                 __fadd2_rn(pp2[e], zz ? rf_zz : rf_zx),
+                                                 zz ? rh_zz : rh_zx, zz ? rl_zz : rl_zx);
+                    const float2 th = __fmul2_rn(t, f2(6.28318530717958647692f));
+                    float sx, cx, sy, cy;
+                    __sincosf(th.x, &sx, &cx);
+                    __sincosf(th.y, &sy, &cy);
+                    // .x: A row r + 32 e (e < 2) or 64 + r (e = 2).
+                    const int ka = zz ? 2 : e;
+                    if (!va[ka]) cx = sx = 0.f;
+                    split16x2(cx, sx, &ah[ka][jj], &al[ka][jj]);
+                    if (zz) {
+                        if (!va[3]) cy = sy = 0.f;
+                        split16x2(cy, sy, &ah[3][jj], &al[3][jj]);
+                    } else {
+                        float wr = 0.f, wi = 0.f;
+                        if (vb[e]) {
+                            wr = v1.z * cy - v1.w * sy;
+                            wi = v1.z * sy + v1.w * cy;
+                        }
+                        split16x2(wr, wi, &bh[e][jj], &bl[e][jj]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t row = (uint32_t)(r + 32 * k);
+                *reinterpret_cast<uint4*>(base + sw128(row, c)) =
+                    make_uint4(ah[k][0], ah[k][1], ah[k][2], ah[k][3]);
+                *reinterpret_cast<uint4*>(base + kPA + sw128(row, c)) =
+                    make_uint4(al[k][0], al[k][1], al[k][2], al[k][3]);
+            }
+            unsigned char* bhi = base + 2 * kPA;
+            unsigned char* blo = bhi + kPB;
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                // Point r + 32 k: (Re W, -Im W) in row r + 32 k, (Im W, Re W)
+                // in row 64 + r + 32 k.
+                const uint32_t row = (uint32_t)(r + 32 * k);
+                *reinterpret_cast<uint4*>(bhi + sw128(row, c)) =
+                    make_uint4(neg_hi(bh[k][0]), neg_hi(bh[k][1]), neg_hi(bh[k][2]), neg_hi(bh[k][3]));
+                *reinterpret_cast<uint4*>(bhi + sw128(64 + row, c)) =
+                    make_uint4(swap_halves(bh[k][0]), swap_halves(bh[k][1]), swap_halves(bh[k][2]),
+                               swap_halves(bh[k][3]));
+                *reinterpret_cast<uint4*>(blo + sw128(row, c)) =
+                    make_uint4(neg_hi(bl[k][0]), neg_hi(bl[k][1]), neg_hi(bl[k][2]), neg_hi(bl[k][3]));
+                *reinterpret_cast<uint4*>(blo + sw128(64 + row, c)) =
+                    make_uint4(swap_halves(bl[k][0]), swap_halves(bl[k][1]), swap_halves(bl[k][2]),
+                               swap_halves(bl[k][3]));
+            }
+            // Make the generic-proxy stores visible to the tensor cores, then
+            // one arrival per warp on the even CTA's stage barrier.
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive_cluster(full_lead + 8u * (uint32_t)s);
+                mbar_arrive(&ray_empty[rb]);
+            }
+        }
+    } else {
+        stage_rays_role(g, lane, rb0, nrb, rays_smem, ray_full, ray_empty, flag);
+    }
+    __syncthreads();
+    if (*flag != 0 && threadIdx.x == 0) atomicExch(g.err, 1);
+    tc_fence_before();
+    cluster_sync();  // the pair MMAs and all cross-CTA arrivals are done
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_free_pair(tmem, 2 * kFN);
     }
 }
 
@@ -523,17 +819,20 @@ __global__ void __launch_bounds__(256) ray_bounds_kernel(const double* __restric
     }
 }
 
+// `group`: x points per real / imaginary column group of a 128-point block
+// (128 for single-CTA tiles, 64 for CTA pairs).
 __global__ void reduce_kernel(const double* __restrict__ partial, int splits, int m_pad, int n_pad,
-                              size_t nz, size_t nx, double scale, double* __restrict__ acc_re,
-                              double* __restrict__ acc_im, int first) {
+                              int group, size_t nz, size_t nx, double scale,
+                              double* __restrict__ acc_re, double* __restrict__ acc_im, int first) {
     const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (idx >= nz * nx) return;
     const size_t iz = idx / nx, ix = idx - iz * nx;
+    const size_t loc = ix & 127, col = (ix >> 7) * kFN + 2 * group * (loc / group) + loc % group;
     double re = 0.0, im = 0.0;
     for (int s = 0; s < splits; ++s) {
-        const double* row = partial + ((size_t)s * m_pad + iz) * n_pad + (ix >> 7) * kFN + (ix & 127);
+        const double* row = partial + ((size_t)s * m_pad + iz) * n_pad + col;
         re += row[0];
-        im += row[128];
+        im += row[group];
     }
     re *= scale;
     im *= scale;
@@ -554,9 +853,12 @@ unsigned grid_1d(size_t n, unsigned threads) { return (unsigned)((n + threads - 
 
 }  // namespace
 
-FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms) {
+FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms, bool allow_pair) {
     FresnelShape sh;
-    sh.m_pad = round_up(std::max<size_t>(nz, 1), 128);
+    // CTA pairs need an even number of 128-row tiles; a screen of at most 128
+    // rows keeps single-CTA tiles rather than padding to 256.
+    sh.pair = allow_pair && nz > 128;
+    sh.m_pad = round_up(std::max<size_t>(nz, 1), sh.pair ? 256 : 128);
     sh.n_pad = round_up(std::max<size_t>(2 * nx, 1), kFN);
     sh.ray_blocks = (int)((n + kFRays - 1) / kFRays);
     sh.tiles = (sh.m_pad / 128) * (sh.n_pad / kFN);
@@ -599,7 +901,7 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
         rep->kernels += 1;
         return Status::Ok();
     }
-    const FresnelShape sh = fresnel_shape(n, nx, nz, num_sms);
+    const FresnelShape sh = fresnel_shape(n, nx, nz, num_sms, ws.allow_pair);
     XK_TRY(ws.partial.ensure((size_t)sh.splits * sh.m_pad * sh.n_pad * sizeof(double)));
     XK_TRY(ws.ctrl.ensure(256));
     static std::once_flag attr_once;
@@ -607,6 +909,10 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     std::call_once(attr_once, [] {
         attr_err = cudaFuncSetAttribute(fresnel_fused_kernel,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmem);
+        if (attr_err == cudaSuccess)
+            attr_err = cudaFuncSetAttribute(fresnel_pair_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kPSmem);
     });
     XK_CUDA_TRY(attr_err);
     int* d_err = ws.ctrl.as<int>();
@@ -635,11 +941,15 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     const dim3 grid((unsigned)(sh.m_pad / 128), (unsigned)(sh.n_pad / kFN), (unsigned)sh.splits);
     const bool timed = rep->ev_gemm[0] && rep->ev_gemm[1];
     if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[0], stream));
-    fresnel_fused_kernel<<<grid, kFThreads, kFSmem, stream>>>(fa);
+    if (sh.pair)  // grid.x is even: m_pad is a multiple of 256
+        fresnel_pair_kernel<<<grid, kPThreads, kPSmem, stream>>>(fa);
+    else
+        fresnel_fused_kernel<<<grid, kFThreads, kFSmem, stream>>>(fa);
     XK_CUDA_TRY(cudaGetLastError());
     if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[1], stream));
     reduce_kernel<<<grid_1d(m, 256), 256, 0, stream>>>(ws.partial.as<double>(), sh.splits,
-                                                        (int)sh.m_pad, (int)sh.n_pad, nz, nx,
+                                                        (int)sh.m_pad, (int)sh.n_pad,
+                                                        sh.pair ? 64 : 128, nz, nx,
                                                         in.max_amp, in.out_re, in.out_im, 1);
     XK_CUDA_TRY(cudaGetLastError());
     rep->kernels += 2;
@@ -766,7 +1076,7 @@ xk::Status fresnel_host(xk_ctx* ctx, const double* rx, const double* rz, const d
         stats->n_tiles = (int)rep.shape.tiles;
         stats->groups = rep.shape.splits;
         stats->n_items = (long long)rep.shape.tiles * rep.shape.splits;
-        stats->sweep = -1;
+        stats->sweep = rep.used_path == XK_PATH_SEPARABLE ? (rep.shape.pair ? 1 : 0) : -1;
     }
     return xk::Status::Ok();
 }

@@ -170,7 +170,8 @@ struct FresnelIn {
 
 struct FresnelShape {
     size_t m_pad = 0, n_pad = 0;  // padded rows of A (screen z) and B (2 x screen x)
-    size_t tiles = 0;             // 128 x 256 output tiles
+    size_t tiles = 0;             // 128 x 256 output tiles (one per CTA)
+    bool pair = false;            // CTA pairs (256 x 256 tiles, one MMA over two SMs)
     int ray_blocks = 0;           // blocks of 32 rays (the contraction)
     int splits = 1;               // K splits per output tile
 };
@@ -178,6 +179,7 @@ struct FresnelShape {
 struct FresnelWorkspace {
     DevBuf coords, partial, ctrl;
     uint32_t wait_limit = 1u << 24;  // polls of every bounded wait of the tensor-core product
+    bool allow_pair = true;          // CTA-pair product on screens of more than 128 rows
 };
 
 struct FresnelReport {
@@ -189,7 +191,7 @@ struct FresnelReport {
     int used_path = 0;                          // XK_PATH_* that ran
 };
 
-FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms);
+FresnelShape fresnel_shape(size_t n, size_t nx, size_t nz, int num_sms, bool allow_pair = true);
 
 // Enqueues screen coordinates into ws.coords (nx then nz doubles; the caller
 // sizes it) and the sum for `path` (XK_PATH_F64 or XK_PATH_SEPARABLE).
