@@ -175,6 +175,11 @@ const char* xk_route_reason(int reason);
  *                    bytes (a positive multiple of 16, at most 1024) beyond its
  *                    copy, so that stage can never complete and the bounded
  *                    wait runs out; cleared after that one execution
+ *   "fresnel_stall"  test hook: 1 makes the next tensor-core Fresnel product on
+ *                    this context arm its first stage's barrier with one
+ *                    arrival more than its producers make, so the MMA issuer's
+ *                    bounded wait runs out (XK_ERR_TIMEOUT); no MMA is issued
+ *                    and nothing stays in flight; cleared after that execution
  *   "fresnel_pair"   XK_PATH_SEPARABLE: 1 (default) computes screens of more
  *                    than 128 rows on CTA pairs (one tcgen05 MMA over two SMs,
  *                    256 x 256 tiles); 0 keeps one CTA per 128 x 256 tile */

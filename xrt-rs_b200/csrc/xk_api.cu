@@ -354,6 +354,9 @@ int xk_set_option(xk_ctx* ctx, const char* name, double value) {
     } else if (n == "fresnel_pair") {
         if (value != 0.0 && value != 1.0) return fail(ctx, XK_ERR_INVALID, "fresnel_pair is 0 or 1");
         ctx->fresnel.allow_pair = value != 0.0;
+    } else if (n == "fresnel_stall") {
+        if (value != 0.0 && value != 1.0) return fail(ctx, XK_ERR_INVALID, "fresnel_stall is 0 or 1");
+        ctx->fresnel.stall_once = (uint32_t)value;
     } else if (n == "inject_stall") {
         if (!(value >= 0.0) || value > 1024.0 || std::fmod(value, 16.0) != 0.0)
             return fail(ctx, XK_ERR_INVALID, "inject_stall must be a multiple of 16 in 0..1024");

@@ -130,10 +130,13 @@ static_assert(kFChunks * (kFProdThreads / kFRowThreads) == 8 && kFRowThreads % 3
 constexpr int kFThreads = 32 + kFEpiThreads + kFProdThreads + 32;  // + the ray stager warp
 constexpr int kFRayBufs = 4;  // staged ray blocks in flight
 constexpr int kFSeg = 20;                        // ray blocks (60 K blocks) per f32 segment
+// Polls of the issuer's final wait for its MMAs (never fewer, whatever the
+// caller's wait limit): the accumulators are freed after it.
+constexpr uint32_t kMmaDrainPolls = 1u << 22;
 constexpr int kFN = 256;                         // accumulator columns (N of the UMMA)
-// Ray staging (two blocks), per ray 8 floats: x hi, x lo, frac(a x^2), z hi,
-// z lo, frac(a z^2) (coordinates relative to the screen centre) and the
-// scaled amplitude.
+// Ray staging (one block per ring buffer), per ray 8 floats: {z hi, x hi,
+// z lo, x lo} and {frac(a z^2), frac(a x^2), es_re, es_im} (coordinates
+// relative to the screen centre, amplitude scaled by 1 / max|es|).
 constexpr uint32_t kFRayBytes = kFRays * 32;
 // Epilogue staging: per epilogue warp 32 rows of 16 FP64 values, rows 144
 // bytes apart (16-byte stores of 32 lanes then meet all banks once).
@@ -154,6 +157,7 @@ struct FusedArgs {
     int m_pad, n_pad;
     int* err;
     uint32_t wait_limit;  // polls of every bounded mbarrier wait
+    uint32_t stall;       // test hook: extra arrivals stage 0's barrier waits for (never made)
 };
 
 // Byte offset of 16-byte chunk c (0..7) of row r in a 128-byte-swizzled tile.
@@ -336,7 +340,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kFStages; ++s) {
-            mbar_init(&full[s], kFProdThreads / 32);  // one arrival per producer warp
+            mbar_init(&full[s], kFProdThreads / 32 + (s == 0 ? g.stall : 0u));  // per producer warp
             mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -397,7 +401,7 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
             // A loop that gave up on a wait may leave MMAs in flight: wait
             // (bounded) for them before the accumulators are freed.
             umma_commit(mma_done);
-            if (!mbar_wait(mma_done, 0, g.wait_limit)) *flag = 1;
+            if (!mbar_wait(mma_done, 0, max(g.wait_limit, kMmaDrainPolls))) *flag = 1;
         }
         __syncwarp();
     } else if (warp <= 4) {
@@ -570,7 +574,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
         // full and acc_empty are used in the even CTA only: they collect the
         // arrivals of both CTAs' producer and epilogue warps.
         for (int s = 0; s < kPStages; ++s) {
-            mbar_init(&full[s], 2 * kPProdThreads / 32);
+            mbar_init(&full[s], 2 * kPProdThreads / 32 + (s == 0 ? g.stall : 0u));
             mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -635,7 +639,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
             // A loop that gave up on a wait may leave MMAs in flight: wait
             // (bounded) for them before either CTA frees its accumulators.
             umma_commit_pair(smem_u32(mma_done));
-            if (!mbar_wait(mma_done, 0, g.wait_limit)) *flag = 1;
+            if (!mbar_wait(mma_done, 0, max(g.wait_limit, kMmaDrainPolls))) *flag = 1;
         }
         __syncwarp();
     } else if (warp <= 4) {
@@ -938,6 +942,8 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     fa.n_pad = (int)sh.n_pad;
     fa.err = d_err;
     fa.wait_limit = ws.wait_limit;
+    fa.stall = ws.stall_once;
+    ws.stall_once = 0;  // armed for one execution
     const dim3 grid((unsigned)(sh.m_pad / 128), (unsigned)(sh.n_pad / kFN), (unsigned)sh.splits);
     const bool timed = rep->ev_gemm[0] && rep->ev_gemm[1];
     if (timed) XK_CUDA_TRY(cudaEventRecord(rep->ev_gemm[0], stream));

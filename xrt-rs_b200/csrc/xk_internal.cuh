@@ -180,6 +180,7 @@ struct FresnelWorkspace {
     DevBuf coords, partial, ctrl;
     uint32_t wait_limit = 1u << 24;  // polls of every bounded wait of the tensor-core product
     bool allow_pair = true;          // CTA-pair product on screens of more than 128 rows
+    uint32_t stall_once = 0;         // test hook: the next product's first stage never completes
 };
 
 struct FresnelReport {
