@@ -216,6 +216,15 @@ __device__ __forceinline__ void split16x2(float a, float b, uint32_t* hi, uint32
     *lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
+// (a + ib)(c + is) with explicit roundings, so that every kernel variant forms
+// the same W bit for bit (no compiler-chosen FMA contraction).
+__device__ __forceinline__ float cmul_re(float a, float b, float c, float s) {
+    return __fmaf_rn(a, c, __fmul_rn(-b, s));
+}
+__device__ __forceinline__ float cmul_im(float a, float b, float c, float s) {
+    return __fmaf_rn(a, s, __fmul_rn(b, c));
+}
+
 // (x, y) -> (x, -y) and (y, x) on packed f16 pairs (sign flip, half swap).
 __device__ __forceinline__ uint32_t neg_hi(uint32_t v) { return v ^ 0x80000000u; }
 __device__ __forceinline__ uint32_t swap_halves(uint32_t v) { return __byte_perm(v, 0, 0x1032); }
@@ -468,8 +477,8 @@ __global__ void __launch_bounds__(kFThreads, 1) fresnel_fused_kernel(FusedArgs g
                         __sincosf(th.y, &sb, &cb);
                         if (!va[k]) ca = sa = 0.f;
                         if (vb[k]) {
-                            wr = v1.z * cb - v1.w * sb;
-                            wi = v1.z * sb + v1.w * cb;
+                            wr = cmul_re(v1.z, v1.w, cb, sb);
+                            wi = cmul_im(v1.z, v1.w, cb, sb);
                         }
                         split16x2(ca, sa, &ah[k][jj], &al[k][jj]);
                         split16x2(wr, wi, &bh[k][jj], &bl[k][jj]);
@@ -537,11 +546,137 @@ constexpr int kPStages = 3;
 constexpr uint32_t kPA = 128 * 128;              // one A tile (hi or lo): 128 rows x 128 B
 constexpr uint32_t kPB = 128 * 128;              // this CTA's half of one B tile
 constexpr uint32_t kPStage = 2 * kPA + 2 * kPB;  // A_hi | A_lo | B_hi | B_lo
-constexpr int kPProdThreads = 256;               // warps 5..12
+constexpr int kPProdThreads = 384;               // warps 5..16
 constexpr int kPThreads = 32 + kFEpiThreads + kPProdThreads + 32;
 constexpr size_t kPSmem =
     1024 + (size_t)kPStages * kPStage + kFRayBufs * kFRayBytes + kFEpiBytes + 256;
 static_assert(kPSmem <= 227 * 1024, "pair kernel shared memory");
+
+// Producer warps of a CTA of the pair. Warps 0..7 (ZZ = false) fill 16-byte
+// chunk c0 = w (rays 4 c0 .. 4 c0 + 3) of the A rows l, l + 32 and of the B
+// rows of x points l, l + 32 (packed pair-rows (A l, B l), (A l+32, B l+32));
+// warps 8..11 (ZZ = true) fill chunks c0, c0 + 1 of the A rows 64 + l, 96 + l
+// (pair-row (A 64+l, A 96+l)). Every thread thus makes 8 packed phase
+// evaluations per ray block; each store instruction of a warp covers 32
+// consecutive rows (no bank conflict). Row z index mt*128 + row, x index
+// nt*128 + 64 half + point.
+template <bool ZZ>
+__device__ __forceinline__ void pair_producer(const FusedArgs& g, int c0, int r, int mt, int nt,
+                                              uint32_t half, int nrb, unsigned char* tiles,
+                                              uint32_t full_lead, uint64_t* empty,
+                                              uint64_t* ray_full, uint64_t* ray_empty,
+                                              unsigned char* rays_smem, volatile int* flag) {
+    using namespace sm100;
+    constexpr int NE = ZZ ? 1 : 2;   // pair-rows per thread
+    constexpr int NCH = ZZ ? 2 : 1;  // chunks per thread
+    bool vx_ok[NE], vy_ok[NE];
+    float2 kh2[NE], khn2[NE], kl2[NE], pp2[NE];
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        // (.x, .y) rows: (A r + 32 e, B r + 32 e) or (A 64 + r, A 96 + r).
+        const size_t izx = (size_t)mt * 128 + (ZZ ? 64 + r : r + 32 * e);
+        vx_ok[e] = izx < g.nz;
+        const double ux = vx_ok[e] ? g.zp[izx] - g.oz : 0.0;
+        double uy;
+        if (ZZ) {
+            const size_t izy = (size_t)mt * 128 + 96 + r;
+            vy_ok[e] = izy < g.nz;
+            uy = vy_ok[e] ? g.zp[izy] - g.oz : 0.0;
+        } else {
+            const size_t ix = (size_t)nt * 128 + 64 * half + r + 32 * e;
+            vy_ok[e] = ix < g.nx;
+            uy = vy_ok[e] ? g.xp[ix] - g.ox : 0.0;
+        }
+        float hx, lx, hy, ly, fx, fy, unused, h0, l0;
+        split_coord(-2.0 * g.a_turns * ux, 0.0, &hx, &lx, &unused);
+        split_coord(-2.0 * g.a_turns * uy, 0.0, &hy, &ly, &unused);
+        split_coord(ux, g.a_turns, &h0, &l0, &fx);
+        split_coord(uy, g.a_turns, &h0, &l0, &fy);
+        kh2[e] = make_float2(hx, hy);
+        khn2[e] = make_float2(-hx, -hy);
+        kl2[e] = make_float2(lx, ly);
+        pp2[e] = make_float2(fx, fy);
+    }
+    for (int i = 0; i < nrb; ++i) {
+        const int s = i % kPStages, rb = i % kFRayBufs;
+        bool ok = mbar_wait(&ray_full[rb], (uint32_t)(i / kFRayBufs) & 1u, g.wait_limit);
+        ok = mbar_wait(&empty[s], ((uint32_t)(i / kPStages) & 1u) ^ 1u, g.wait_limit) && ok;
+        if (!ok) *flag = 1;
+        unsigned char* base = tiles + (size_t)s * kPStage;
+        unsigned char* bhi = base + 2 * kPA;
+        unsigned char* blo = bhi + kPB;
+        const float4* sr = reinterpret_cast<const float4*>(rays_smem + rb * kFRayBytes);
+#pragma unroll
+        for (int ch = 0; ch < NCH; ++ch) {
+            const int c = c0 + ch;
+            // [row][ray]: A rows of .x and (ZZ) of .y; B points of .y.
+            uint32_t ah[2][4], al[2][4], bh[2][4], bl[2][4];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const int j = 4 * c + jj;
+                const float4 v0 = sr[2 * j], v1 = sr[2 * j + 1];
+                const float2 rh = ZZ ? f2(v0.x) : make_float2(v0.x, v0.y);
+                const float2 rl = ZZ ? f2(v0.z) : make_float2(v0.z, v0.w);
+                const float2 rf = ZZ ? f2(v1.x) : make_float2(v1.x, v1.y);
+#pragma unroll
+                for (int e = 0; e < NE; ++e) {
+                    const float2 t = pair_turns2(kh2[e], khn2[e], kl2[e], __fadd2_rn(pp2[e], rf), rh, rl);
+                    const float2 th = __fmul2_rn(t, f2(6.28318530717958647692f));
+                    float sx, cx, sy, cy;
+                    __sincosf(th.x, &sx, &cx);
+                    __sincosf(th.y, &sy, &cy);
+                    if (!vx_ok[e]) cx = sx = 0.f;
+                    split16x2(cx, sx, &ah[ZZ ? 0 : e][jj], &al[ZZ ? 0 : e][jj]);
+                    if (ZZ) {
+                        if (!vy_ok[e]) cy = sy = 0.f;
+                        split16x2(cy, sy, &ah[1][jj], &al[1][jj]);
+                    } else {
+                        float wr = 0.f, wi = 0.f;
+                        if (vy_ok[e]) {
+                            wr = cmul_re(v1.z, v1.w, cy, sy);
+                            wi = cmul_im(v1.z, v1.w, cy, sy);
+                        }
+                        split16x2(wr, wi, &bh[e][jj], &bl[e][jj]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t row = (uint32_t)(ZZ ? 64 + r + 32 * k : r + 32 * k);
+                *reinterpret_cast<uint4*>(base + sw128(row, c)) =
+                    make_uint4(ah[k][0], ah[k][1], ah[k][2], ah[k][3]);
+                *reinterpret_cast<uint4*>(base + kPA + sw128(row, c)) =
+                    make_uint4(al[k][0], al[k][1], al[k][2], al[k][3]);
+            }
+            if (!ZZ) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    // Point r + 32 k: (Re W, -Im W) in row r + 32 k, (Im W,
+                    // Re W) in row 64 + r + 32 k.
+                    const uint32_t row = (uint32_t)(r + 32 * k);
+                    *reinterpret_cast<uint4*>(bhi + sw128(row, c)) = make_uint4(
+                        neg_hi(bh[k][0]), neg_hi(bh[k][1]), neg_hi(bh[k][2]), neg_hi(bh[k][3]));
+                    *reinterpret_cast<uint4*>(bhi + sw128(64 + row, c)) =
+                        make_uint4(swap_halves(bh[k][0]), swap_halves(bh[k][1]),
+                                   swap_halves(bh[k][2]), swap_halves(bh[k][3]));
+                    *reinterpret_cast<uint4*>(blo + sw128(row, c)) = make_uint4(
+                        neg_hi(bl[k][0]), neg_hi(bl[k][1]), neg_hi(bl[k][2]), neg_hi(bl[k][3]));
+                    *reinterpret_cast<uint4*>(blo + sw128(64 + row, c)) =
+                        make_uint4(swap_halves(bl[k][0]), swap_halves(bl[k][1]),
+                                   swap_halves(bl[k][2]), swap_halves(bl[k][3]));
+                }
+            }
+        }
+        // Make the generic-proxy stores visible to the tensor cores, then one
+        // arrival per warp on the even CTA's stage barrier.
+        fence_proxy_async();
+        __syncwarp();
+        if (r == 0) {
+            mbar_arrive_cluster(full_lead + 8u * (uint32_t)s);
+            mbar_arrive(&ray_empty[rb]);
+        }
+    }
+}
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     fresnel_pair_kernel(FusedArgs g) {
@@ -649,126 +784,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
             mbar_arrive_cluster(acc_empty_lead + 8u * (uint32_t)b);
         });
     } else if (warp < 5 + kPProdThreads / 32) {
-        // Producers: warp w' = warp - 5 fills 16-byte chunk c = w' (rays
-        // 4c .. 4c+3) of every row; lane l computes the A rows l, l + 32,
-        // 64 + l, 96 + l (screen z index mt*128 + row) and the x points l,
-        // l + 32 of this CTA's half (screen x index nt*128 + 64 half + point).
-        // Three packed phase evaluations per ray: (A l, B l), (A l+32, B l+32)
-        // and (A 64+l, A 96+l). Each store instruction of a warp covers 32
-        // consecutive rows (no bank conflict).
-        const int c = warp - 5;
-        const int r = lane;
-        bool va[4], vb[2];
-        float2 kh2[3], khn2[3], kl2[3], pp2[3];
-        {
-            double zr[4], xr[2];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const size_t iz = (size_t)mt * 128 + r + 32 * k;
-                va[k] = iz < g.nz;
-                zr[k] = va[k] ? g.zp[iz] - g.oz : 0.0;
-            }
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const size_t ix = (size_t)nt * 128 + 64 * half + r + 32 * k;
-                vb[k] = ix < g.nx;
-                xr[k] = vb[k] ? g.xp[ix] - g.ox : 0.0;
-            }
-            // Pair-row e: (.x, .y) = (z row, x point) for e = 0, 1 and (z row,
-            // z row) for e = 2.
-            const double ux[3] = {zr[0], zr[1], zr[2]}, uy[3] = {xr[0], xr[1], zr[3]};
-#pragma unroll
-            for (int e = 0; e < 3; ++e) {
-                float hx, lx, hy, ly, fx, fy, unused, h0, l0;
-                split_coord(-2.0 * g.a_turns * ux[e], 0.0, &hx, &lx, &unused);
-                split_coord(-2.0 * g.a_turns * uy[e], 0.0, &hy, &ly, &unused);
-                split_coord(ux[e], g.a_turns, &h0, &l0, &fx);
-                split_coord(uy[e], g.a_turns, &h0, &l0, &fy);
-                kh2[e] = make_float2(hx, hy);
-                khn2[e] = make_float2(-hx, -hy);
-                kl2[e] = make_float2(lx, ly);
-                pp2[e] = make_float2(fx, fy);
-            }
-        }
+        const int w = warp - 5;
         const uint32_t full_lead = mapa_shared(full, 0);
-        for (int i = 0; i < nrb; ++i) {
-            const int s = i % kPStages, rb = i % kFRayBufs;
-            bool ok = mbar_wait(&ray_full[rb], (uint32_t)(i / kFRayBufs) & 1u, g.wait_limit);
-            ok = mbar_wait(&empty[s], ((uint32_t)(i / kPStages) & 1u) ^ 1u, g.wait_limit) && ok;
-            if (!ok) *flag = 1;
-            unsigned char* base = tiles + (size_t)s * kPStage;
-            const float4* sr = reinterpret_cast<const float4*>(rays_smem + rb * kFRayBytes);
-            uint32_t ah[4][4], al[4][4], bh[2][4], bl[2][4];
-#pragma unroll
-            for (int jj = 0; jj < 4; ++jj) {
-                const int j = 4 * c + jj;
-                const float4 v0 = sr[2 * j], v1 = sr[2 * j + 1];
-                // Ray terms of the (z, x) and (z, z) pair-rows.
-                const float2 rh_zx = make_float2(v0.x, v0.y), rl_zx = make_float2(v0.z, v0.w);
-                const float2 rf_zx = make_float2(v1.x, v1.y);
-                const float2 rh_zz = f2(v0.x), rl_zz = f2(v0.z), rf_zz = f2(v1.x);
-#pragma unroll
-                for (int e = 0; e < 3; ++e) {
-                    const bool zz = e == 2;
-                    const float2 t = pair_turns2(kh2[e], khn2[e], kl2[e],
-                                                 __fadd2_rn(pp2[e], zz ? rf_zz : rf_zx),
-                                                 zz ? rh_zz : rh_zx, zz ? rl_zz : rl_zx);
-                    const float2 th = __fmul2_rn(t, f2(6.28318530717958647692f));
-                    float sx, cx, sy, cy;
-                    __sincosf(th.x, &sx, &cx);
-                    __sincosf(th.y, &sy, &cy);
-                    // .x: A row r + 32 e (e < 2) or 64 + r (e = 2).
-                    const int ka = zz ? 2 : e;
-                    if (!va[ka]) cx = sx = 0.f;
-                    split16x2(cx, sx, &ah[ka][jj], &al[ka][jj]);
-                    if (zz) {
-                        if (!va[3]) cy = sy = 0.f;
-                        split16x2(cy, sy, &ah[3][jj], &al[3][jj]);
-                    } else {
-                        float wr = 0.f, wi = 0.f;
-                        if (vb[e]) {
-                            wr = v1.z * cy - v1.w * sy;
-                            wi = v1.z * sy + v1.w * cy;
-                        }
-                        split16x2(wr, wi, &bh[e][jj], &bl[e][jj]);
-                    }
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const uint32_t row = (uint32_t)(r + 32 * k);
-                *reinterpret_cast<uint4*>(base + sw128(row, c)) =
-                    make_uint4(ah[k][0], ah[k][1], ah[k][2], ah[k][3]);
-                *reinterpret_cast<uint4*>(base + kPA + sw128(row, c)) =
-                    make_uint4(al[k][0], al[k][1], al[k][2], al[k][3]);
-            }
-            unsigned char* bhi = base + 2 * kPA;
-            unsigned char* blo = bhi + kPB;
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                // Point r + 32 k: (Re W, -Im W) in row r + 32 k, (Im W, Re W)
-                // in row 64 + r + 32 k.
-                const uint32_t row = (uint32_t)(r + 32 * k);
-                *reinterpret_cast<uint4*>(bhi + sw128(row, c)) =
-                    make_uint4(neg_hi(bh[k][0]), neg_hi(bh[k][1]), neg_hi(bh[k][2]), neg_hi(bh[k][3]));
-                *reinterpret_cast<uint4*>(bhi + sw128(64 + row, c)) =
-                    make_uint4(swap_halves(bh[k][0]), swap_halves(bh[k][1]), swap_halves(bh[k][2]),
-                               swap_halves(bh[k][3]));
-                *reinterpret_cast<uint4*>(blo + sw128(row, c)) =
-                    make_uint4(neg_hi(bl[k][0]), neg_hi(bl[k][1]), neg_hi(bl[k][2]), neg_hi(bl[k][3]));
-                *reinterpret_cast<uint4*>(blo + sw128(64 + row, c)) =
-                    make_uint4(swap_halves(bl[k][0]), swap_halves(bl[k][1]), swap_halves(bl[k][2]),
-                               swap_halves(bl[k][3]));
-            }
-            // Make the generic-proxy stores visible to the tensor cores, then
-            // one arrival per warp on the even CTA's stage barrier.
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive_cluster(full_lead + 8u * (uint32_t)s);
-                mbar_arrive(&ray_empty[rb]);
-            }
-        }
+        if (w < 8)
+            pair_producer<false>(g, w, lane, mt, nt, half, nrb, tiles, full_lead, empty, ray_full,
+                                 ray_empty, rays_smem, flag);
+        else
+            pair_producer<true>(g, 2 * (w - 8), lane, mt, nt, half, nrb, tiles, full_lead, empty,
+                                ray_full, ray_empty, rays_smem, flag);
     } else {
         stage_rays_role(g, lane, rb0, nrb, rays_smem, ray_full, ray_empty, flag);
     }
