@@ -131,7 +131,9 @@ def test_cta_pair_tiles_match_single_cta_tiles(ctx, oracle, shape):
     """Screens of more than 128 rows run the product on CTA pairs (one tcgen05
     MMA over two SMs, 256 x 256 tiles, option "fresnel_pair" = 1, the
     default); "fresnel_pair" = 0 keeps one CTA per 128 x 256 tile. Both match
-    the oracle, and each other to within the f32 accumulation order."""
+    the oracle and each other: bit for bit where both pad the screen to the same
+    rows (and so split K the same way), else to the FP64 summation order of the
+    K splits."""
     nx, nz = shape
     x, z, es = rays(3000, seed=31 + nx)
     sc = FresnelScreen(-0.3, 0.3, nx, -0.25, 0.2, nz)
