@@ -252,7 +252,9 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        # The same scaling key as this arm's CUDA line for the same flags.
+        "higher_is_better": True, "scaling": "strong" if args.shard == "screen" else "weak",
+        "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": single_workload(args.rays, args.grid), "rays": args.rays,
                    "screen_points": args.grid ** 2,
