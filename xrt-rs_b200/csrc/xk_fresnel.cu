@@ -931,17 +931,14 @@ Status fresnel_enqueue(const FresnelIn& in, FresnelWorkspace& ws, cudaStream_t s
     const FresnelShape sh = fresnel_shape(n, nx, nz, num_sms, ws.allow_pair);
     XK_TRY(ws.partial.ensure((size_t)sh.splits * sh.m_pad * sh.n_pad * sizeof(double)));
     XK_TRY(ws.ctrl.ensure(256));
-    static std::once_flag attr_once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(fresnel_fused_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmem);
-        if (attr_err == cudaSuccess)
-            attr_err = cudaFuncSetAttribute(fresnel_pair_kernel,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)kPSmem);
-    });
-    XK_CUDA_TRY(attr_err);
+    // Set on every call: the attribute belongs to the current device's
+    // context, and a process may use several devices.
+    if (sh.pair)
+        XK_CUDA_TRY(cudaFuncSetAttribute(fresnel_pair_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmem));
+    else
+        XK_CUDA_TRY(cudaFuncSetAttribute(fresnel_fused_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmem));
     int* d_err = ws.ctrl.as<int>();
     XK_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
     FusedArgs fa;
