@@ -100,6 +100,9 @@ def parse():
                     help="serve: pairs per epoch (0 = the server's default)")
     ap.add_argument("--item-pairs", type=float, default=0.0,
                     help="serve: pairs per work item (0 = the server's default)")
+    ap.add_argument("--serve-policy", type=int, default=0, choices=[0, 1],
+                    help="server epoch sharing: 0 shortest remaining work first, aged "
+                         "(default); 1 equal share per running request")
     ap.add_argument("--reserve-sms", type=int, default=0,
                     help="serve: SMs left to planning (0 = the server's default)")
     ap.add_argument("--shard", choices=["screen", "replica"], default="screen",
@@ -567,7 +570,8 @@ def run_fresnel(args):
 
 
 def serve_session(ctx, rate_hz: float, duration_s: float, drain_s: float, seed: int = 0,
-                  epoch_pairs: float = 0.0, item_pairs: float = 0.0, reserve_sms: int = 0):
+                  epoch_pairs: float = 0.0, item_pairs: float = 0.0, reserve_sms: int = 0,
+                  policy: int = 0):
     """One Poisson request stream through the continuous-batching server.
 
     Request sizes follow the serving configuration (rays log-uniform in
@@ -587,7 +591,7 @@ def serve_session(ctx, rate_hz: float, duration_s: float, drain_s: float, seed: 
     reqs = synth.config4_requests(seed=seed, rate_hz=rate_hz, duration_s=duration_s)
     base = synth.gaussian_aperture(2_000_000, 0.1, 10_000.0, 30_000.0, seed=1)
     srv = Server(ctx, hbm_budget_bytes=120e9, epoch_pairs=epoch_pairs,
-                 item_pairs=item_pairs, reserve_sms=reserve_sms)
+                 item_pairs=item_pairs, reserve_sms=reserve_sms, policy=policy)
     sets = {}
     lat, done_pairs, failures = [], [0.0], [0]
     lock = threading.Lock()
@@ -692,7 +696,8 @@ def run_serve(args):
     torch.cuda.set_device(0)
     ctx = xrt_rs.GpuContext.new(0)
     res = serve_session(ctx, args.rate, args.duration, args.drain, epoch_pairs=args.epoch_pairs,
-                        item_pairs=args.item_pairs, reserve_sms=args.reserve_sms)
+                        item_pairs=args.item_pairs, reserve_sms=args.reserve_sms,
+                        policy=args.serve_policy)
     ctx.close()
     line = {"workload": "serve", "metric": "served latency and throughput", **res,
             "data": "synthetic: rays sliced from one 2e6-ray aperture, square-grid screens"}
@@ -967,12 +972,16 @@ def main():
     # 200 req/s (about 8x what one B200 computes), each for a bounded window.
     serve = None
     if rank == 0 and world == 1 and not args.no_serve:
-        sust = serve_session(ctx, args.serve_rate, args.serve_window, 10.0, seed=0)
-        over = serve_session(ctx, 200.0, args.serve_window, 10.0, seed=1)
+        sust = serve_session(ctx, args.serve_rate, args.serve_window, 10.0, seed=0,
+                             policy=args.serve_policy)
+        over = serve_session(ctx, 200.0, args.serve_window, 10.0, seed=1,
+                             policy=args.serve_policy)
         serve = {
             "mix": "rays log-uniform [1e4, 2e6], screen points log-uniform [256, 1e6], "
                    "E ~ U(1, 30) keV, d ~ U(100, 20000) mm, 30 % resident ray sets, "
                    "HBM budget 120 GB, FP32 phase-reduced",
+            "policy": ("equal share per running request" if args.serve_policy == 1 else
+                       "shortest remaining work first, aged (1 s)"),
             "p99_ms": sust["p99_ms"], "sustainable": sust, "offered_200_req_s": over}
         if fp64:
             # The FP64 path serves at most its single-solve rate: the offered

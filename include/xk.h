@@ -419,7 +419,17 @@ typedef struct xk_server_opts {
     double item_pairs;                /* target pairs per work item; 0 = 1e6 */
     int inject_alloc_failure_every;   /* testing: fail every k-th request allocation; 0 = off */
     int reserve_sms;                  /* SMs epochs leave free for planning kernels; 0 = 8 */
+    int policy;                       /* how an epoch's pair budget is shared among running
+                                         requests: XK_SERVE_SHORTEST_AGED (0, default) fills it in
+                                         order of remaining pairs / (1 + waited / aging_ms), so
+                                         small requests finish in few epochs and the wait of
+                                         large ones stays bounded; XK_SERVE_EQUAL_SHARE (1) gives
+                                         every running request the same share */
+    double aging_ms;                  /* aging constant of XK_SERVE_SHORTEST_AGED; 0 = 1000 */
 } xk_server_opts;
+
+#define XK_SERVE_SHORTEST_AGED 0
+#define XK_SERVE_EQUAL_SHARE 1
 
 typedef struct xk_request {
     xk_rays rays;       /* host pointers; ignored when rayset != 0 */

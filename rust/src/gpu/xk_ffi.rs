@@ -24,6 +24,8 @@ pub const XK_ERR_SHUTDOWN: c_int = 9;
 pub const XK_PATH_F64: c_int = 0;
 pub const XK_PATH_F32PR: c_int = 1;
 pub const XK_PATH_SEPARABLE: c_int = 2;
+pub const XK_SERVE_SHORTEST_AGED: c_int = 0;
+pub const XK_SERVE_EQUAL_SHARE: c_int = 1;
 
 pub const XK_BATCH_DEVICE: c_int = 1;
 pub const XK_BATCH_NO_GRAPH: c_int = 2;
@@ -240,6 +242,8 @@ pub struct xk_server_opts {
     pub item_pairs: f64,
     pub inject_alloc_failure_every: c_int,
     pub reserve_sms: c_int,
+    pub policy: c_int,
+    pub aging_ms: f64,
 }
 
 #[repr(C)]

@@ -13,7 +13,7 @@ import pytest
 
 import cases
 import xrt_rs
-from xrt_rs import synth
+from xrt_rs import XkError, _lib, synth
 from xrt_rs.serve import Server
 
 pytestmark = pytest.mark.gpu
@@ -46,6 +46,32 @@ def test_results_match_oracle_and_are_mix_independent(ctx, oracle):
         exact = oracle.kahan_ld(*cases.as_lists(rays, pix))
         assert cases.rel_l2(b, exact) < PR_TOL, i
     srv.close()
+
+
+@pytest.mark.parametrize("policy", [0, 1])
+def test_results_do_not_depend_on_the_policy(ctx, policy):
+    """Both epoch-sharing policies (aged shortest-remaining-first, equal
+    share) give every request the same field, bit for bit, as a request served
+    alone: the policy decides only when a request's work items run."""
+    reqs = small_requests(seed=12, count=6)
+    ref_srv = Server(ctx, epoch_pairs=5e8, policy=1)
+    alone = []
+    for rays, pix in reqs:
+        alone.append(tuple(a.copy() for a in ref_srv.wait(ref_srv.submit(pix, rays=rays))))
+    ref_srv.close()
+    srv = Server(ctx, epoch_pairs=3e8, policy=policy, aging_ms=50.0)
+    tickets = [srv.submit(pix, rays=rays) for rays, pix in reqs]
+    for i, (t, a) in enumerate(zip(tickets, alone)):
+        b = srv.wait(t)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), f"request {i} differs under policy {policy}"
+    srv.close()
+
+
+def test_unknown_policy_is_rejected(ctx):
+    with pytest.raises(XkError) as ei:
+        Server(ctx, policy=7)
+    assert ei.value.code == _lib.XK_ERR_INVALID
 
 
 def test_requests_overlap_on_the_device(ctx):

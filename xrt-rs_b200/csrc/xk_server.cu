@@ -341,18 +341,43 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
     s->next_slot = (s->next_slot + 1) % kEpochRing;
     retire_slot(s, e);
 
-    const double share = s->opts.epoch_pairs / std::max<size_t>(1, runnable.size());
     struct Take {
         Req* q;
         long long first, count;
     };
     std::vector<Take> takes;
-    for (Req* q : runnable) {
-        long long quota = (long long)std::max(1.0, std::floor(share / std::max(1.0, q->pairs_per_item)));
+    auto take = [&](Req* q, double pairs) {
+        long long quota = (long long)std::max(1.0, std::floor(pairs / std::max(1.0, q->pairs_per_item)));
         quota = std::min(quota, q->slice_cap);
         quota = std::min(quota, q->n_items - q->next_item);
-        if (quota <= 0) continue;
+        if (quota <= 0) return 0.0;
         takes.push_back({q, q->next_item, quota});
+        return (double)quota * q->pairs_per_item;
+    };
+    if (s->opts.policy == XK_SERVE_EQUAL_SHARE) {
+        // Every running request gets the same share of the epoch's pairs.
+        const double share = s->opts.epoch_pairs / std::max<size_t>(1, runnable.size());
+        for (Req* q : runnable) take(q, share);
+    } else {
+        // Shortest remaining work first, aged: the epoch's pairs go to the
+        // requests in order of remaining pairs / (1 + waited / aging_ms).
+        // Small requests leave in few epochs; a large one's key halves each
+        // aging_ms it waits, so it is not starved.
+        const Clock::time_point now = Clock::now();
+        std::vector<std::pair<double, Req*>> order;
+        order.reserve(runnable.size());
+        for (Req* q : runnable) {
+            const double left = (double)(q->n_items - q->next_item) * q->pairs_per_item;
+            const double waited = ms_between(q->t_submit, now);
+            order.push_back({left / (1.0 + waited / s->opts.aging_ms), q});
+        }
+        std::stable_sort(order.begin(), order.end(),
+                         [](const auto& a, const auto& b) { return a.first < b.first; });
+        double budget = s->opts.epoch_pairs;
+        for (const auto& o : order) {
+            if (budget <= 0.0) break;
+            budget -= take(o.second, budget);
+        }
     }
     if (takes.empty()) return xk::Status::Ok();
 
@@ -641,6 +666,9 @@ xk::Status create_server(xk_ctx* ctx, const xk_server_opts* opts, xk_server** ou
     if (s->opts.max_active <= 0) s->opts.max_active = 64;
     if (s->opts.item_pairs <= 0) s->opts.item_pairs = 1e6;
     if (s->opts.reserve_sms <= 0) s->opts.reserve_sms = 8;
+    if (s->opts.policy != XK_SERVE_SHORTEST_AGED && s->opts.policy != XK_SERVE_EQUAL_SHARE)
+        return xk::Status::Err(XK_ERR_INVALID, "unknown serving policy");
+    if (s->opts.aging_ms <= 0) s->opts.aging_ms = 1000.0;
     s->opts.reserve_sms = std::min(s->opts.reserve_sms, s->num_sms - 1);
     s->pr_opts = ctx->pr_opts;
     // Keep freed stream-ordered memory in the pool instead of returning it to

@@ -26,6 +26,8 @@ XK_ERR_SHUTDOWN = 9
 XK_PATH_F64 = 0
 XK_PATH_F32PR = 1
 XK_PATH_SEPARABLE = 2
+XK_SERVE_SHORTEST_AGED = 0
+XK_SERVE_EQUAL_SHARE = 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -130,7 +132,8 @@ XK_BATCH_NO_GRAPH = 2
 class XkServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_double), ("epoch_pairs", ctypes.c_double),
                 ("max_active", ctypes.c_int), ("item_pairs", ctypes.c_double),
-                ("inject_alloc_failure_every", ctypes.c_int), ("reserve_sms", ctypes.c_int)]
+                ("inject_alloc_failure_every", ctypes.c_int), ("reserve_sms", ctypes.c_int),
+                ("policy", ctypes.c_int), ("aging_ms", ctypes.c_double)]
 
 
 class XkRequest(ctypes.Structure):

@@ -25,12 +25,13 @@ from . import (PIXEL_FIELDS, RAY_FIELDS, XkError, _check_lengths, _f64, _path, _
 
 class Server:
     def __init__(self, ctx=None, hbm_budget_bytes=0.0, epoch_pairs=0.0, max_active=0,
-                 item_pairs=0.0, inject_alloc_failure_every=0, reserve_sms=0, log=None):
+                 item_pairs=0.0, inject_alloc_failure_every=0, reserve_sms=0, log=None,
+                 policy=0, aging_ms=0.0):
         self._ctx = _require_ctx(ctx)
         self._log = open(log, "a") if log else None
         opts = _lib.XkServerOpts(float(hbm_budget_bytes), float(epoch_pairs), int(max_active),
                                  float(item_pairs), int(inject_alloc_failure_every),
-                                 int(reserve_sms))
+                                 int(reserve_sms), int(policy), float(aging_ms))
         h = ctypes.c_void_p()
         _lib.check(_lib.load().xk_server_create(self._ctx.handle, ctypes.byref(opts),
                                                 ctypes.byref(h)), self._ctx.handle)
