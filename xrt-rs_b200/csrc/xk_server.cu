@@ -4,10 +4,11 @@
 // them:
 //   * the scheduler admits requests while the admitted set fits an HBM
 //     budget and the slot count, and launches epochs: each epoch is one
-//     persistent launch over work items of every planned request — a fair
-//     share of the epoch's pair budget each — so requests that arrive while
-//     others are on the GPU join the next epoch and run on the device
-//     together with the older ones. Up to three epochs are queued, and epochs
+//     persistent launch over work items of the planned requests — its pair
+//     budget filled in order of remaining work aged by waiting time (or an
+//     equal share each, as an option) — so requests that arrive while others
+//     are on the GPU join the next epoch and run on the device together with
+//     the older ones. Up to three epochs are queued, and epochs
 //     leave a few SMs free so that planning kernels never wait behind them;
 //   * the planner copies the inputs of newly admitted requests (or uses a
 //     resident ray set) and plans all of them in one batched pass on a
