@@ -8,7 +8,7 @@
 //     budget filled in order of remaining work aged by waiting time (or an
 //     equal share each, as an option) — so requests that arrive while others
 //     are on the GPU join the next epoch and run on the device together with
-//     the older ones. Up to three epochs are queued, and epochs
+//     the older ones. Up to two epochs are queued, and epochs
 //     leave a few SMs free so that planning kernels never wait behind them;
 //   * the planner copies the inputs of newly admitted requests (or uses a
 //     resident ray set) and plans all of them in one batched pass on a
@@ -79,7 +79,9 @@ struct Req {
     RaySet* rayset = nullptr;
 };
 
-constexpr int kEpochRing = 3;
+// Epochs queued on the device at once: one running and one ready keep the GPU
+// busy; a third only delays new requests by one more epoch.
+constexpr int kEpochRing = 2;
 constexpr int kVariants = xk::kPrVariants;
 constexpr int kForkStreams = 4;  // streams the kernel variants of one epoch run on
 constexpr int kPlanBatch = 32;  // requests planned together at most
