@@ -364,8 +364,9 @@ xk::Status run_epoch(xk_server* s, std::vector<Req*>& runnable) {
     } else {
         // Shortest remaining work first, aged: the epoch's pairs go to the
         // requests in order of remaining pairs / (1 + waited / aging_ms).
-        // Small requests leave in few epochs; a large one's key halves each
-        // aging_ms it waits, so it is not starved.
+        // Small requests leave in few epochs; a large one's key shrinks as it
+        // waits (half after aging_ms, a third after twice that), so it is not
+        // starved.
         const Clock::time_point now = Clock::now();
         std::vector<std::pair<double, Req*>> order;
         order.reserve(runnable.size());
