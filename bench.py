@@ -229,22 +229,24 @@ def run_reference(args):
     rays, screen = synth.config1(seed=0, n_rays=args.rays, grid=args.grid)
     rl = [rays[k] for k in ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re",
                             "ep_im", "energy")]
-    threads = oracle.max_threads()
+    # All the host's cores: rank 0 runs alone (torchrun sets OMP_NUM_THREADS=1
+    # for every rank, which would otherwise leave the reference on one core).
+    threads = max(oracle.max_threads(), len(os.sched_getaffinity(0)))
     # Size one step to ~2 s of CPU work.
     sub, _ = synth.subsample_screen(screen, 16, seed=7)
     t0 = time.perf_counter()
-    oracle.kahan_f64(rl, [sub["x"], sub["y"], sub["z"]])
+    oracle.kahan_f64(rl, [sub["x"], sub["y"], sub["z"]], threads=threads)
     per_point = (time.perf_counter() - t0) / 16
     count = int(max(16, min(len(screen["x"]), 2.0 / max(per_point, 1e-6))))
     count = balanced_count(count, threads, len(screen["x"]))
     sub, _ = synth.subsample_screen(screen, count, seed=7)
     pl = [sub["x"], sub["y"], sub["z"]]
     for _ in range(args.warmup):
-        oracle.kahan_f64(rl, pl)
+        oracle.kahan_f64(rl, pl, threads=threads)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        oracle.kahan_f64(rl, pl)
+        oracle.kahan_f64(rl, pl, threads=threads)
         times.append(time.perf_counter() - t0)
     ms = 1e3 * float(np.mean(times))
     pairs = len(rl[0]) * count
