@@ -194,13 +194,13 @@ def cpu_baseline(rays, screen, seconds: float):
 
     rl = [rays[k] for k in ("x", "y", "z", "nx", "ny", "nz", "nl", "es_re", "es_im", "ep_re",
                             "ep_im", "energy")]
-    threads = oracle.max_threads()
+    threads = max(oracle.max_threads(), len(os.sched_getaffinity(0)))  # not torchrun's 1
     count = balanced_count(8, threads, len(screen["x"]))
     rate = None
     while True:
         sub, _ = synth.subsample_screen(screen, count, seed=7)
         t0 = time.perf_counter()
-        oracle.kahan_f64(rl, [sub["x"], sub["y"], sub["z"]])
+        oracle.kahan_f64(rl, [sub["x"], sub["y"], sub["z"]], threads=threads)
         dt = time.perf_counter() - t0
         rate = len(rl[0]) * count / dt
         if dt >= seconds * 0.5 or count >= len(screen["x"]):
