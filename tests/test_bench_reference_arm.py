@@ -56,3 +56,6 @@ def test_reference_arm_under_torchrun_two_ranks():
     lines = _json_lines(r.stdout)
     assert len(lines) == 1
     _check(lines[0])
+    # Rank 0 works alone: it uses every host core, whatever OMP_NUM_THREADS
+    # the launcher set.
+    assert lines[0]["cpu_baseline"]["cores"] >= len(os.sched_getaffinity(0))
